@@ -1,0 +1,209 @@
+/*
+ * ohm.h - C ABI of the B200-native Ohmnivore hot path (libohm_b200.so).
+ *
+ * This library replaces the reference's per-Newton-iteration solver layer
+ * (the src/solver/ Rust modules of winstanley-industries/ohmnivore): device evaluation and
+ * MNA stamping, CSR SpMV, and BiCGSTAB with Jacobi or ISAI(1)
+ * preconditioning, run as persistent sm_100a kernels.  Every entry point
+ * takes plain pointers and sizes; host arrays are caller-owned, device
+ * objects are owned by the context that created them.
+ *
+ * Threading: a context is single-threaded, like the reference's backends
+ * (src/solver/backend.rs:205-209 hold Cell counters and are not Sync).
+ * Errors: every call returns an ohm_status; ohm_last_error() gives the text
+ * of the last failure on the calling thread.  No call aborts the process.
+ */
+#ifndef OHM_H
+#define OHM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: OhmnivoreError (src/error.rs:4-33) ------------------ */
+typedef enum {
+    OHM_OK = 0,
+    OHM_ERR_SOLVE = 1,                 /* OhmnivoreError::Solve (breakdown, no convergence, singular) */
+    OHM_ERR_NEWTON_NOT_CONVERGED = 2,  /* OhmnivoreError::NewtonNotConverged{iterations, max_residual} */
+    OHM_ERR_NEWTON_NUMERICAL = 3,      /* OhmnivoreError::NewtonNumericalError{iteration} */
+    OHM_ERR_COMPILE = 4,               /* OhmnivoreError::Compile (descriptor / CSR validation) */
+    OHM_ERR_TIMEOUT = 5,               /* a bounded device wait gave up (no OhmnivoreError twin) */
+    OHM_ERR_INVALID_ARG = 6,           /* bad pointer, size or parameter */
+    OHM_ERR_CUDA = 7,                  /* CUDA runtime failure */
+    OHM_ERR_TIMESTEP = 8               /* OhmnivoreError::Timestep */
+} ohm_status;
+
+/* Detail code of an OHM_ERR_SOLVE from the Krylov solver; the status words of
+ * the reference's fused kernel (src/solver/ds_backend.rs:71-76) plus the
+ * breakdown kinds of src/solver/bicgstab.rs:107-182. */
+typedef enum {
+    OHM_KRYLOV_RUNNING = 0,
+    OHM_KRYLOV_CONVERGED = 1,
+    OHM_KRYLOV_MAXITER = 2,            /* "did not converge within N iterations" */
+    OHM_KRYLOV_BREAKDOWN_RHO = 3,      /* "breakdown: rho ~ 0" */
+    OHM_KRYLOV_BREAKDOWN_RV = 4,       /* "breakdown: r_hat.v ~ 0" */
+    OHM_KRYLOV_BREAKDOWN_TT = 5,       /* "breakdown: ||t|| ~ 0" */
+    OHM_KRYLOV_BREAKDOWN_OMEGA = 6,    /* "breakdown: omega ~ 0" */
+    OHM_KRYLOV_NAN = 7                 /* "diverged: NaN/Inf in residual" */
+} ohm_krylov_code;
+
+typedef enum {
+    OHM_PREC_FP64 = 0,   /* FP64 Krylov (the plain path) */
+    OHM_PREC_MIXED = 1   /* FP32 Krylov bulk, FP64 dots, FP64 residual / Newton update */
+} ohm_precision;
+
+typedef enum {
+    OHM_PRECOND_AUTO = 0,    /* block Jacobi: 1x1, 2x2 for zero-diagonal branch rows paired with
+                                their node row, identity for unpaired zero-diagonal rows */
+    OHM_PRECOND_JACOBI = 1,  /* reference Jacobi: 1/a_ii, 0 where |a_ii| <= 1e-30 (gpu.rs:177-190) */
+    OHM_PRECOND_ISAI1 = 2,   /* ISAI(1) from ILU(0) factors, z = M_U (M_L r) (gpu.rs:139-168) */
+    OHM_PRECOND_NONE = 3
+} ohm_precond;
+
+/* ---- device descriptors: byte-identical to src/compiler.rs:46-149 ------- */
+typedef struct {                 /* GpuDiodeDescriptor, 48 bytes */
+    uint32_t anode_idx, cathode_idx;
+    float is_val, n_vt;
+    uint32_t g_row_col[4];       /* [aa, cc, ac, ca] CSR value indices, UINT32_MAX = ground */
+    uint32_t b_idx[2];           /* [anode, cathode] */
+    uint32_t padding[2];
+} ohm_diode_desc;
+
+typedef struct {                 /* GpuBjtDescriptor, 96 bytes */
+    uint32_t collector_idx, base_idx, emitter_idx;
+    float polarity, is_val, bf, br, nf_vt, nr_vt;
+    uint32_t node_fixed[3];
+    uint32_t g_row_col[9];       /* [CC, CB, CE, BC, BB, BE, EC, EB, EE] */
+    uint32_t b_idx[3];           /* [C, B, E] */
+} ohm_bjt_desc;
+
+typedef struct {                 /* GpuMosfetDescriptor, 64 bytes */
+    uint32_t drain_idx, gate_idx, source_idx;
+    float polarity, vto, kp, lambda;
+    uint32_t node_fixed_packed;  /* bit0 drain, bit1 gate, bit2 source */
+    uint32_t g_row_col[6];       /* [DD, DG, DS, SD, SG, SS] */
+    uint32_t b_idx[2];           /* [D, S] */
+} ohm_mosfet_desc;
+
+/* ---- parameters --------------------------------------------------------- */
+typedef struct {                 /* BiCgStabParams (src/solver/bicgstab.rs:14-27) + extensions */
+    int32_t max_iterations;      /* default 10000 (bicgstab.rs:10) */
+    double tolerance;            /* ||r|| < tolerance * ||b||, default 1e-5 (bicgstab.rs:11) */
+    int32_t precision;           /* ohm_precision */
+    int32_t precond;             /* ohm_precond */
+    double inner_rtol;           /* mixed: inner FP32 solve also stops at inner_rtol*||r0||; 0 = off */
+    int32_t max_refinements;     /* mixed: FP64 iterative-refinement sweeps (>= 1) */
+    int32_t max_restarts;        /* restarts with r_hat = r after a rho or r_hat.v breakdown;
+                                    0 = the reference's breakdown error; default 50 */
+} ohm_krylov_params;
+
+typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + extensions */
+    int32_t max_iterations;      /* default 50 */
+    double abs_tol;              /* converged when max|x - x_old| < abs_tol (+ rel_tol*max|x|); default 1e-4 */
+    double rel_tol;              /* extension, default 0 */
+    ohm_krylov_params krylov;    /* linear sub-solve; reference default tolerance 1e-5 */
+    const double *initial_guess; /* NewtonParams::initial_guess, host pointer, may be NULL */
+} ohm_newton_params;
+
+typedef struct {
+    int32_t status;              /* ohm_status of the solve */
+    int32_t krylov_code;         /* ohm_krylov_code of the last linear solve */
+    int32_t iterations;          /* Newton iterations (or Krylov iterations for linear solves) */
+    int32_t error_iteration;     /* NewtonNumericalError{iteration} */
+    int64_t krylov_iterations;   /* total BiCGSTAB iterations */
+    double max_residual;         /* last max|x - x_old| (NewtonNotConverged{max_residual}) */
+    double final_residual_norm;  /* ||b - A x||_2 at exit (FP64), when computed */
+    double b_norm;               /* ||b||_2 of the last linear system */
+    int64_t kernel_launches;     /* kernels this call launched */
+} ohm_solve_info;
+
+/* Reference defaults; fill before changing fields. */
+void ohm_krylov_params_default(ohm_krylov_params *p);
+void ohm_newton_params_default(ohm_newton_params *p);
+
+/* ---- context ------------------------------------------------------------ */
+typedef struct ohm_ctx ohm_ctx;
+typedef struct ohm_buf ohm_buf;      /* SolverBackend::Buffer: FP64 device vector */
+typedef struct ohm_csr ohm_csr;      /* GpuCsrMatrix: device CSR (u32 indices, FP64 values) */
+typedef struct ohm_plan ohm_plan;    /* device-resident nonlinear system (Newton plan) */
+
+const char *ohm_last_error(void);
+const char *ohm_version(void);
+
+/* One context = one CUDA device + one stream (WgpuDsBackend::new, ds_backend.rs). */
+ohm_status ohm_ctx_create(int device, ohm_ctx **out);
+ohm_status ohm_ctx_destroy(ohm_ctx *ctx);
+ohm_status ohm_ctx_synchronize(ohm_ctx *ctx);
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void *ohm_ctx_stream(ohm_ctx *ctx);
+
+/* ---- SolverBackend (src/solver/backend.rs:51-96) ------------------------ */
+ohm_status ohm_buf_create(ohm_ctx *ctx, int64_t n, ohm_buf **out);            /* new_buffer (zeroed) */
+ohm_status ohm_buf_destroy(ohm_buf *buf);
+ohm_status ohm_buf_upload(ohm_ctx *ctx, ohm_buf *buf, const double *host, int64_t n);   /* upload_vec */
+ohm_status ohm_buf_download(ohm_ctx *ctx, const ohm_buf *buf, double *host, int64_t n); /* download_vec */
+double *ohm_buf_device_ptr(ohm_buf *buf);
+ohm_status ohm_csr_upload(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *row_ptr,
+                          const uint32_t *col, const double *values, ohm_csr **out); /* upload_matrix */
+ohm_status ohm_csr_update_values(ohm_ctx *ctx, ohm_csr *m, const double *values, int64_t nnz);
+ohm_status ohm_csr_destroy(ohm_csr *m);
+ohm_status ohm_spmv(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *x, ohm_buf *y);       /* spmv */
+ohm_status ohm_dot(ohm_ctx *ctx, const ohm_buf *a, const ohm_buf *b, double *out);      /* dot -> f64 */
+ohm_status ohm_axpy(ohm_ctx *ctx, double alpha, const ohm_buf *x, ohm_buf *y);          /* y += a x */
+ohm_status ohm_copy(ohm_ctx *ctx, const ohm_buf *src, ohm_buf *dst);                    /* copy */
+ohm_status ohm_scale(ohm_ctx *ctx, double alpha, ohm_buf *x);                            /* scale */
+
+/* ---- LinearSolver::solve_real (src/solver/mod.rs:27-34, gpu.rs:107-208) --
+ * Host CSR (u32 indices as uploaded by gpu.rs:124-125) and host b / x.
+ * x is written on success.  Runs right-preconditioned BiCGSTAB
+ * (bicgstab.rs:56-189) as one persistent kernel. */
+ohm_status ohm_solve_real(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *row_ptr,
+                          const uint32_t *col, const double *values, const double *b,
+                          double *x, const ohm_krylov_params *params, ohm_solve_info *info);
+
+/* Same on device-resident operands (no host copies). */
+ohm_status ohm_solve_real_device(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *b, ohm_buf *x,
+                                 const ohm_krylov_params *params, ohm_solve_info *info);
+
+/* ---- newton_solve (src/solver/newton.rs:65-78) ---------------------------
+ * Argument order follows the reference.  x_out receives the solution
+ * (size entries).  The whole Newton loop (evaluate, stamp, solve, limit,
+ * converge) runs on the device as one persistent kernel. */
+ohm_status ohm_newton_solve(ohm_ctx *ctx, const double *base_g_values, const uint32_t *col_indices,
+                            const uint32_t *row_ptrs, const double *base_b,
+                            const ohm_diode_desc *diodes, int64_t n_diodes,
+                            const ohm_bjt_desc *bjts, int64_t n_bjts,
+                            const ohm_mosfet_desc *mosfets, int64_t n_mosfets,
+                            int64_t size, int64_t nnz, const ohm_newton_params *params,
+                            double *x_out, ohm_solve_info *info);
+
+/* Device-resident Newton plan: uploads the system once, runs many solves.
+ * bjt_vaf: optional per-BJT Early voltage (extension, NULL or +inf = none). */
+ohm_status ohm_plan_create(ohm_ctx *ctx, const double *base_g_values, const uint32_t *col_indices,
+                           const uint32_t *row_ptrs, const double *base_b,
+                           const ohm_diode_desc *diodes, int64_t n_diodes,
+                           const ohm_bjt_desc *bjts, int64_t n_bjts,
+                           const ohm_mosfet_desc *mosfets, int64_t n_mosfets,
+                           const double *bjt_vaf, int64_t size, int64_t nnz, ohm_plan **out);
+ohm_status ohm_plan_destroy(ohm_plan *plan);
+/* Replace base values / base rhs (e.g. GMIN stepping, a new timestep). NULL keeps. */
+ohm_status ohm_plan_set_base(ohm_plan *plan, const double *base_g_values, const double *base_b);
+/* Run Newton.  x_inout: device pointer (size doubles) holding the initial
+ * guess (if params->initial_guess is NULL the device x is used as is) and
+ * receiving the solution. */
+ohm_status ohm_plan_newton_device(ohm_plan *plan, double *x_inout_device,
+                                  const ohm_newton_params *params, ohm_solve_info *info);
+/* Device-side system matrix / rhs of the last assembly (for tests). */
+ohm_status ohm_plan_download_system(ohm_plan *plan, double *values, double *rhs);
+/* Evaluate + stamp at x (host), return J values and b_eq (host): one assembly. */
+ohm_status ohm_plan_assemble(ohm_plan *plan, const double *x_host, double *values_out, double *rhs_out);
+/* One limiting step: x_new_inout (host) is damped against x_old (host). */
+ohm_status ohm_plan_limit(ohm_plan *plan, const double *x_old_host, double *x_new_inout);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OHM_H */

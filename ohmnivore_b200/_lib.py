@@ -1,0 +1,123 @@
+"""ctypes binding of ``libohm_b200.so`` (declared in ``include/ohm.h``).
+
+The shared library is built in-tree by ``ohmnivore_b200/csrc/Makefile``.
+There is no fallback: importing the solver without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libohm_b200.so")
+
+# ohm_status
+OK, ERR_SOLVE, ERR_NEWTON_NOT_CONVERGED, ERR_NEWTON_NUMERICAL, ERR_COMPILE, ERR_TIMEOUT, \
+    ERR_INVALID_ARG, ERR_CUDA, ERR_TIMESTEP = range(9)
+PREC_FP64, PREC_MIXED = 0, 1
+PRECOND_AUTO, PRECOND_JACOBI, PRECOND_ISAI1, PRECOND_NONE = 0, 1, 2, 3
+
+
+class KrylovParams(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("tolerance", C.c_double), ("precision", C.c_int32),
+                ("precond", C.c_int32), ("inner_rtol", C.c_double), ("max_refinements", C.c_int32),
+                ("max_restarts", C.c_int32)]
+
+
+class NewtonParamsC(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
+                ("krylov", KrylovParams), ("initial_guess", C.POINTER(C.c_double))]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("krylov_code", C.c_int32), ("iterations", C.c_int32),
+                ("error_iteration", C.c_int32), ("krylov_iterations", C.c_int64),
+                ("max_residual", C.c_double), ("final_residual_norm", C.c_double),
+                ("b_norm", C.c_double), ("kernel_launches", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = C.c_void_p
+_i64 = C.c_int64
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "ohm_last_error": (C.c_char_p, []),
+    "ohm_version": (C.c_char_p, []),
+    "ohm_krylov_params_default": (None, [C.POINTER(KrylovParams)]),
+    "ohm_newton_params_default": (None, [C.POINTER(NewtonParamsC)]),
+    "ohm_ctx_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "ohm_ctx_destroy": (C.c_int, [_vp]),
+    "ohm_ctx_synchronize": (C.c_int, [_vp]),
+    "ohm_ctx_stream": (_vp, [_vp]),
+    "ohm_buf_create": (C.c_int, [_vp, _i64, C.POINTER(_vp)]),
+    "ohm_buf_destroy": (C.c_int, [_vp]),
+    "ohm_buf_upload": (C.c_int, [_vp, _vp, _dp, _i64]),
+    "ohm_buf_download": (C.c_int, [_vp, _vp, _dp, _i64]),
+    "ohm_buf_device_ptr": (_vp, [_vp]),
+    "ohm_csr_upload": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, C.POINTER(_vp)]),
+    "ohm_csr_update_values": (C.c_int, [_vp, _vp, _dp, _i64]),
+    "ohm_csr_destroy": (C.c_int, [_vp]),
+    "ohm_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ohm_dot": (C.c_int, [_vp, _vp, _vp, _dp]),
+    "ohm_axpy": (C.c_int, [_vp, C.c_double, _vp, _vp]),
+    "ohm_copy": (C.c_int, [_vp, _vp, _vp]),
+    "ohm_scale": (C.c_int, [_vp, C.c_double, _vp]),
+    "ohm_solve_real": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp,
+                                 C.POINTER(KrylovParams), C.POINTER(SolveInfo)]),
+    "ohm_solve_real_device": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(KrylovParams),
+                                        C.POINTER(SolveInfo)]),
+    "ohm_newton_solve": (C.c_int, [_vp, _dp, _u32p, _u32p, _dp, _vp, _i64, _vp, _i64, _vp, _i64,
+                                   _i64, _i64, C.POINTER(NewtonParamsC), _dp, C.POINTER(SolveInfo)]),
+    "ohm_plan_create": (C.c_int, [_vp, _dp, _u32p, _u32p, _dp, _vp, _i64, _vp, _i64, _vp, _i64, _dp,
+                                  _i64, _i64, C.POINTER(_vp)]),
+    "ohm_plan_destroy": (C.c_int, [_vp]),
+    "ohm_plan_set_base": (C.c_int, [_vp, _dp, _dp]),
+    "ohm_plan_newton_device": (C.c_int, [_vp, _vp, C.POINTER(NewtonParamsC), C.POINTER(SolveInfo)]),
+    "ohm_plan_download_system": (C.c_int, [_vp, _dp, _dp]),
+    "ohm_plan_assemble": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "ohm_plan_limit": (C.c_int, [_vp, _dp, _dp]),
+}
+
+_LIB = None
+
+
+def load():
+    """Load the library (once).  Raises if it is missing or lacks a symbol."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `make -C ohmnivore_b200/csrc` "
+                          "or __graft_entry__.build()")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().ohm_last_error().decode(errors="replace")
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def u32ptr(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_u32p)
+
+
+def vptr(a):
+    return None if a is None or len(a) == 0 else C.c_void_p(a.ctypes.data)

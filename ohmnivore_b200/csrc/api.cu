@@ -1,0 +1,844 @@
+// C ABI of libohm_b200: contexts, device buffers (SolverBackend), the linear
+// solve (LinearSolver::solve_real) and the device-resident Newton plan
+// (newton_solve).  Host-side work here is validation, the stamp map and the
+// preconditioner structure; all arithmetic runs in the persistent kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+using namespace ohm;
+
+static_assert(sizeof(ohm_diode_desc) == sizeof(DiodeDesc), "diode layout");
+static_assert(sizeof(ohm_bjt_desc) == sizeof(BjtDesc), "bjt layout");
+static_assert(sizeof(ohm_mosfet_desc) == sizeof(MosfetDesc), "mosfet layout");
+
+// ----------------------------------------------------------------- errors --
+static thread_local std::string g_last_error;
+
+ohm_status ohm_fail(ohm_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+#define fail ohm_fail
+
+extern "C" const char *ohm_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *ohm_version(void) { return "ohm_b200 0.1 (sm_100a)"; }
+
+extern "C" void ohm_krylov_params_default(ohm_krylov_params *p) {
+    if (!p) return;
+    p->max_iterations = 10000;        // bicgstab.rs:10
+    p->tolerance = 1e-5;              // bicgstab.rs:11
+    p->precision = OHM_PREC_FP64;
+    p->precond = OHM_PRECOND_AUTO;
+    p->inner_rtol = 0.0;
+    p->max_refinements = 1;
+    p->max_restarts = 50;
+}
+
+extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
+    if (!p) return;
+    p->max_iterations = 50;           // newton.rs:48
+    p->abs_tol = 1e-4;                // newton.rs:49
+    p->rel_tol = 0.0;
+    ohm_krylov_params_default(&p->krylov);
+    p->initial_guess = nullptr;
+}
+
+// ---------------------------------------------------------------- context --
+extern "C" ohm_status ohm_ctx_create(int device, ohm_ctx **out) {
+    if (!out) return fail(OHM_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(OHM_ERR_INVALID_ARG, "device %d out of range (%d)", device, ndev);
+    CUDA_TRY(cudaSetDevice(device));
+    int coop = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop) return fail(OHM_ERR_CUDA, "device %d lacks cooperative launch", device);
+    ohm_ctx *c = new (std::nothrow) ohm_ctx();
+    if (!c) return fail(OHM_ERR_INVALID_ARG, "out of host memory");
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = dalloc(&c->sync_words, 4);
+    if (e == cudaSuccess) e = dalloc(&c->info_dev, 1);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->info_host, sizeof(DeviceInfo));
+    if (e == cudaSuccess) e = dalloc(&c->dot_scratch, 2048);
+    if (e != cudaSuccess) {
+        ohm_ctx_destroy(c);
+        return fail(OHM_ERR_CUDA, "context setup failed: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_ctx_destroy(ohm_ctx *c) {
+    if (!c) return OHM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->sync_words);
+    cudaFree(c->info_dev);
+    cudaFreeHost(c->info_host);
+    cudaFree(c->dot_scratch);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_ctx_synchronize(ohm_ctx *c) {
+    if (!c) return fail(OHM_ERR_INVALID_ARG, "ctx is null");
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return OHM_OK;
+}
+
+extern "C" void *ohm_ctx_stream(ohm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+// ------------------------------------------------------------- validation --
+static ohm_status check_csr(int64_t n, int64_t nnz, const uint32_t *rp, const uint32_t *col) {
+    if (n < 0 || nnz < 0) return fail(OHM_ERR_INVALID_ARG, "negative size");
+    if (n > 0x7fffffffLL || nnz > 0xfffffffeLL) return fail(OHM_ERR_INVALID_ARG, "size exceeds u32 indexing");
+    if (!rp || (nnz > 0 && !col)) return fail(OHM_ERR_INVALID_ARG, "null CSR pointer");
+    if (rp[0] != 0) return fail(OHM_ERR_COMPILE, "row_ptr[0] = %u, expected 0", rp[0]);
+    for (int64_t i = 0; i < n; ++i)
+        if (rp[i + 1] < rp[i]) return fail(OHM_ERR_COMPILE, "row_ptr decreases at row %lld", (long long)i);
+    if ((int64_t)rp[n] != nnz) return fail(OHM_ERR_COMPILE, "row_ptr[n] = %u != nnz %lld", rp[n], (long long)nnz);
+    for (int64_t k = 0; k < nnz; ++k)
+        if ((int64_t)col[k] >= n) return fail(OHM_ERR_COMPILE, "column index %u out of range at %lld", col[k], (long long)k);
+    return OHM_OK;
+}
+
+static inline bool idx_ok(uint32_t v, int64_t lim) { return v == kSentinel || (int64_t)v < lim; }
+
+static ohm_status check_devices(const ohm_diode_desc *d, int64_t nd, const ohm_bjt_desc *q, int64_t nq,
+                                const ohm_mosfet_desc *m, int64_t nm, int64_t size, int64_t nnz) {
+    if (nd < 0 || nq < 0 || nm < 0) return fail(OHM_ERR_INVALID_ARG, "negative device count");
+    if ((nd && !d) || (nq && !q) || (nm && !m)) return fail(OHM_ERR_INVALID_ARG, "null descriptor array");
+    for (int64_t k = 0; k < nd; ++k) {
+        const ohm_diode_desc &x = d[k];
+        bool ok = idx_ok(x.anode_idx, size) && idx_ok(x.cathode_idx, size);
+        for (int j = 0; j < 4; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
+        for (int j = 0; j < 2; ++j) ok = ok && idx_ok(x.b_idx[j], size);
+        if (!ok) return fail(OHM_ERR_COMPILE, "diode %lld has an index out of range", (long long)k);
+    }
+    for (int64_t k = 0; k < nq; ++k) {
+        const ohm_bjt_desc &x = q[k];
+        bool ok = idx_ok(x.collector_idx, size) && idx_ok(x.base_idx, size) && idx_ok(x.emitter_idx, size);
+        for (int j = 0; j < 9; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
+        for (int j = 0; j < 3; ++j) ok = ok && idx_ok(x.b_idx[j], size);
+        if (!ok) return fail(OHM_ERR_COMPILE, "BJT %lld has an index out of range", (long long)k);
+    }
+    for (int64_t k = 0; k < nm; ++k) {
+        const ohm_mosfet_desc &x = m[k];
+        bool ok = idx_ok(x.drain_idx, size) && idx_ok(x.gate_idx, size) && idx_ok(x.source_idx, size);
+        for (int j = 0; j < 6; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
+        for (int j = 0; j < 2; ++j) ok = ok && idx_ok(x.b_idx[j], size);
+        if (!ok) return fail(OHM_ERR_COMPILE, "MOSFET %lld has an index out of range", (long long)k);
+    }
+    return OHM_OK;
+}
+
+// --------------------------------------------------- preconditioner setup --
+// Block-Jacobi structure.  Rows whose diagonal is structurally zero (voltage
+// source and inductor branch rows of an MNA matrix, src/compiler.rs:376-408)
+// are paired with the off-diagonal column of largest magnitude whose row is
+// unpaired and has a usable diagonal; the 2x2 block [[a_jj a_jk][a_kj 0]] has
+// det = -a_jk a_kj != 0.  Unpaired zero-diagonal rows keep the reference's
+// Jacobi rule (inverse 0).  `touched` marks diagonal slots the device stamps
+// change; those rows never count as zero-diagonal.
+struct PcHost {
+    std::vector<int32_t> partner;
+    std::vector<uint32_t> diag_slot, off_slot;
+};
+
+static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, const double *val,
+                          const std::vector<char> &touched_slot, bool pairs, PcHost &pc) {
+    pc.partner.assign(n, -1);
+    pc.diag_slot.assign(n, kSentinel);
+    pc.off_slot.assign(n, kSentinel);
+    for (int64_t i = 0; i < n; ++i)
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if ((int64_t)col[k] == i) { pc.diag_slot[i] = k; break; }
+    if (!pairs) return;
+    auto zero_diag = [&](int64_t i) {
+        const uint32_t s = pc.diag_slot[i];
+        if (s == kSentinel) return true;
+        if (!touched_slot.empty() && touched_slot[s]) return false;
+        return std::fabs(val[s]) <= 1e-30;
+    };
+    auto slot_of = [&](int64_t r, int64_t c) -> uint32_t {
+        for (uint32_t k = rp[r]; k < rp[r + 1]; ++k)
+            if ((int64_t)col[k] == c) return k;
+        return kSentinel;
+    };
+    for (int64_t k = 0; k < n; ++k) {
+        if (!zero_diag(k) || pc.partner[k] >= 0) continue;
+        int64_t best = -1;
+        double best_mag = 0.0;
+        uint32_t best_kj = kSentinel, best_jk = kSentinel;
+        for (uint32_t e = rp[k]; e < rp[k + 1]; ++e) {
+            const int64_t j = col[e];
+            if (j == k || pc.partner[j] >= 0 || zero_diag(j)) continue;
+            const double mag = std::fabs(val[e]);
+            if (!(mag > 0.0)) continue;
+            const uint32_t jk = slot_of(j, k);
+            if (jk == kSentinel || !(std::fabs(val[jk]) > 0.0)) continue;
+            if (mag > best_mag) { best_mag = mag; best = j; best_kj = e; best_jk = jk; }
+        }
+        if (best >= 0) {
+            pc.partner[k] = (int32_t)best;
+            pc.partner[best] = (int32_t)k;
+            pc.off_slot[k] = best_kj;
+            pc.off_slot[best] = best_jk;
+        }
+    }
+}
+
+// ------------------------------------------------------------ launch logic --
+using KernelFn = void (*)(KernelArgs);
+
+template <typename T>
+static KernelFn pick_kernel(int lpr) {
+    switch (lpr) {
+        case 1: return persistent_solver<T, 1>;
+        case 2: return persistent_solver<T, 2>;
+        case 4: return persistent_solver<T, 4>;
+        case 8: return persistent_solver<T, 8>;
+        case 16: return persistent_solver<T, 16>;
+        default: return persistent_solver<T, 32>;
+    }
+}
+
+static int choose_lpr(int64_t n, int64_t nnz) {
+    const double avg = n > 0 ? (double)nnz / (double)n : 1.0;
+    if (avg <= 2.5) return 1;
+    if (avg <= 5.5) return 2;
+    if (avg <= 12.0) return 4;
+    if (avg <= 24.0) return 8;
+    if (avg <= 48.0) return 16;
+    return 32;
+}
+
+static constexpr int kBlock = 512;
+
+static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, bool mixed, int64_t nnz, int *launches) {
+    const int lpr = choose_lpr(a.n, nnz);
+    KernelFn fn = mixed ? pick_kernel<float>(lpr) : pick_kernel<double>(lpr);
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+    if (per_sm < 1) return fail(OHM_ERR_CUDA, "solver kernel does not fit on an SM");
+    per_sm = std::min(per_sm, 2);
+    int64_t want = (a.n + kBlock - 1) / kBlock;
+    const int64_t ndev = (int64_t)a.nd + a.nq + a.nm;
+    want = std::max<int64_t>(want, (ndev + kBlock - 1) / kBlock);
+    int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
+    a.gs.count = c->sync_words;
+    a.gs.gen = c->sync_words + 1;
+    a.gs.error = (int *)(c->sync_words + 2);
+    a.info = c->info_dev;
+    CUDA_TRY(cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->info_dev, 0, sizeof(DeviceInfo), c->stream));
+    void *args[] = {&a};
+    CUDA_TRY(cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kBlock), args, 0, c->stream));
+    if (launches) *launches += 1;
+    return OHM_OK;
+}
+
+static ohm_status finish_solver(ohm_ctx *c, ohm_solve_info *info, int launches) {
+    unsigned int words[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(c->info_host, c->info_dev, sizeof(DeviceInfo), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const DeviceInfo &di = *c->info_host;
+    ohm_status st = OHM_OK;
+    if (words[2] != 0) {
+        st = fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
+    } else {
+        switch (di.status) {
+            case kOk: st = OHM_OK; break;
+            case kErrSolve: {
+                static const char *why[] = {"running", "converged", "did not converge within the iteration limit",
+                                            "breakdown: rho ~ 0", "breakdown: r_hat.v ~ 0",
+                                            "breakdown: ||t|| ~ 0", "breakdown: omega ~ 0",
+                                            "diverged: NaN/Inf in residual"};
+                const int k = (di.krylov_code >= 0 && di.krylov_code <= 7) ? di.krylov_code : 0;
+                st = fail(OHM_ERR_SOLVE, "BiCGSTAB %s", why[k]);
+                break;
+            }
+            case kErrNewtonNotConverged:
+                st = fail(OHM_ERR_NEWTON_NOT_CONVERGED,
+                          "Newton solver did not converge after %d iterations (max residual: %.2e)",
+                          di.iterations, di.max_residual);
+                break;
+            case kErrNewtonNumerical:
+                st = fail(OHM_ERR_NEWTON_NUMERICAL, "Newton solver encountered numerical error at iteration %d",
+                          di.error_iteration);
+                break;
+            default: st = fail(OHM_ERR_CUDA, "unknown device status %d", di.status);
+        }
+    }
+    if (info) {
+        info->status = st;
+        info->krylov_code = di.krylov_code;
+        info->iterations = di.iterations;
+        info->error_iteration = di.error_iteration;
+        info->krylov_iterations = di.krylov_iterations;
+        info->max_residual = di.max_residual;
+        info->final_residual_norm = di.final_residual;
+        info->b_norm = di.b_norm;
+        info->kernel_launches = launches;
+    }
+    return st;
+}
+
+// Krylov workspace shared by the linear solve and the Newton plan: ten
+// vectors of 8-byte slots (large enough for either precision), the FP64
+// residual, preconditioner coefficients, and the reduction partials.
+struct Workspace {
+    int64_t n = 0;
+    double *vec = nullptr;       // 12 * n doubles
+    double *r64 = nullptr;
+    double *partials = nullptr;  // 8 * max grid
+    int32_t *partner = nullptr;
+    uint32_t *diag_slot = nullptr, *off_slot = nullptr;
+    void release() {
+        cudaFree(vec); cudaFree(r64); cudaFree(partials);
+        cudaFree(partner); cudaFree(diag_slot); cudaFree(off_slot);
+        vec = r64 = partials = nullptr; partner = nullptr; diag_slot = off_slot = nullptr;
+    }
+    cudaError_t alloc(int64_t n_, int num_sms) {
+        n = n_;
+        cudaError_t e = dalloc(&vec, 12 * (size_t)n);
+        if (e == cudaSuccess) e = dalloc(&r64, n);
+        if (e == cudaSuccess) e = dalloc(&partials, 8 * (size_t)num_sms * 8);
+        if (e == cudaSuccess) e = dalloc(&partner, n);
+        if (e == cudaSuccess) e = dalloc(&diag_slot, n);
+        if (e == cudaSuccess) e = dalloc(&off_slot, n);
+        return e;
+    }
+    void bind(KernelArgs &a) const {
+        void **slots[] = {&a.r, &a.rhat, &a.p0, &a.p1, &a.v, &a.s, &a.t, &a.phat, &a.shat, &a.d,
+                          &a.pc_self, &a.pc_part};
+        for (int k = 0; k < 12; ++k) *slots[k] = (void *)(vec + (size_t)k * n);
+        a.r64 = r64;
+        a.partials = partials;
+        a.partner = partner;
+        a.diag_slot = diag_slot;
+        a.off_slot = off_slot;
+    }
+    cudaError_t upload_pc(const PcHost &pc, cudaStream_t s) {
+        cudaError_t e = cudaMemcpyAsync(partner, pc.partner.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(diag_slot, pc.diag_slot.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(off_slot, pc.off_slot.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        return e;
+    }
+};
+
+static ohm_status check_krylov(const ohm_krylov_params *p) {
+    if (!p) return fail(OHM_ERR_INVALID_ARG, "params is null");
+    if (p->max_iterations <= 0) return fail(OHM_ERR_SOLVE, "BiCGSTAB max_iterations must be > 0");
+    if (!(p->tolerance > 0.0) || !std::isfinite(p->tolerance))
+        return fail(OHM_ERR_SOLVE, "BiCGSTAB tolerance must be finite and > 0");
+    if (p->precision != OHM_PREC_FP64 && p->precision != OHM_PREC_MIXED)
+        return fail(OHM_ERR_INVALID_ARG, "unknown precision %d", p->precision);
+    if (p->precond < 0 || p->precond > OHM_PRECOND_NONE)
+        return fail(OHM_ERR_INVALID_ARG, "unknown preconditioner %d", p->precond);
+    if (p->precond == OHM_PRECOND_ISAI1)
+        return fail(OHM_ERR_INVALID_ARG, "ISAI(1) is not available in this build");
+    return OHM_OK;
+}
+
+__global__ void f64_to_f32_kernel(const double *in, float *out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+// -------------------------------------------------------- linear solves --
+static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *d_rp, const uint32_t *d_col,
+                                  double *d_val, const uint32_t *h_rp, const uint32_t *h_col, const double *h_val,
+                                  double *d_b, double *d_x, const ohm_krylov_params *p, ohm_solve_info *info) {
+    const bool mixed = p->precision == OHM_PREC_MIXED;
+    Workspace ws;
+    float *v32 = nullptr;
+    int launches = 0;
+    ohm_status st = OHM_OK;
+    cudaError_t e = ws.alloc(n, c->num_sms);
+    if (e == cudaSuccess && mixed) e = dalloc(&v32, nnz);
+    if (e != cudaSuccess) { ws.release(); cudaFree(v32); return fail(OHM_ERR_CUDA, "workspace: %s", cudaGetErrorString(e)); }
+    PcHost pc;
+    build_precond(n, h_rp, h_col, h_val, {}, p->precond == OHM_PRECOND_AUTO, pc);
+    e = ws.upload_pc(pc, c->stream);
+    if (e == cudaSuccess && mixed && nnz > 0) {
+        f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, c->stream>>>(d_val, v32, nnz);
+        e = cudaGetLastError();
+        ++launches;
+    }
+    if (e != cudaSuccess) { ws.release(); cudaFree(v32); return fail(OHM_ERR_CUDA, "setup: %s", cudaGetErrorString(e)); }
+    KernelArgs a{};
+    a.n = (int)n; a.nnz = (int)nnz;
+    a.row_ptr = d_rp; a.col = d_col; a.vals64 = d_val; a.vals32 = v32;
+    a.b = d_b; a.x = d_x;
+    a.precond = p->precond == OHM_PRECOND_NONE ? kPcNone : (p->precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
+    ws.bind(a);
+    a.newton = 0;
+    a.max_outer = mixed ? std::max(1, p->max_refinements) : 1;
+    a.max_krylov = p->max_iterations;
+    a.krylov_tol = p->tolerance;
+    a.inner_rtol = mixed ? (p->inner_rtol > 0.0 ? p->inner_rtol : 1e-4) : p->inner_rtol;
+    a.accept_partial = mixed ? 1 : 0;
+    a.require_true_residual = mixed ? 1 : 0;
+    a.max_restarts = std::max(0, p->max_restarts);
+    st = launch_solver(c, a, mixed, nnz, &launches);
+    if (st == OHM_OK) st = finish_solver(c, info, launches);
+    cudaStreamSynchronize(c->stream);
+    ws.release();
+    cudaFree(v32);
+    return st;
+}
+
+extern "C" ohm_status ohm_solve_real(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *row_ptr, const uint32_t *col,
+                                     const double *values, const double *b, double *x, const ohm_krylov_params *params,
+                                     ohm_solve_info *info) {
+    if (!c) return fail(OHM_ERR_INVALID_ARG, "ctx is null");
+    ohm_status st = check_krylov(params);
+    if (st != OHM_OK) return st;
+    if (n == 0) return OHM_OK;                       // cpu.rs:39-41, gpu.rs:118-120
+    if (!b || !x || (nnz && !values)) return fail(OHM_ERR_INVALID_ARG, "null array");
+    st = check_csr(n, nnz, row_ptr, col);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaSetDevice(c->device));
+    uint32_t *d_rp = nullptr, *d_col = nullptr;
+    double *d_val = nullptr, *d_b = nullptr, *d_x = nullptr;
+    cudaError_t e = dalloc(&d_rp, n + 1);
+    if (e == cudaSuccess) e = dalloc(&d_col, nnz);
+    if (e == cudaSuccess) e = dalloc(&d_val, nnz);
+    if (e == cudaSuccess) e = dalloc(&d_b, n);
+    if (e == cudaSuccess) e = dalloc(&d_x, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rp, row_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_col, col, nnz * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_val, values, nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_x, 0, n * sizeof(double), c->stream);
+    if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    if (st == OHM_OK) st = solve_real_impl(c, n, nnz, d_rp, d_col, d_val, row_ptr, col, values, d_b, d_x, params, info);
+    if (st == OHM_OK) {
+        e = cudaMemcpyAsync(x, d_x, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_b); cudaFree(d_x);
+    return st;
+}
+
+// ------------------------------------------------------------ Newton plan --
+struct ohm_plan {
+    ohm_ctx *ctx = nullptr;
+    int64_t n = 0, nnz = 0, nd = 0, nq = 0, nm = 0;
+    uint32_t *rp = nullptr, *col = nullptr;
+    double *base_vals = nullptr, *vals64 = nullptr, *base_b = nullptr, *b = nullptr;
+    float *vals32 = nullptr;
+    double *x_prev = nullptr, *x_scratch = nullptr;
+    DiodeDesc *diodes = nullptr;
+    BjtDesc *bjts = nullptr;
+    MosfetDesc *mosfets = nullptr;
+    double *vaf = nullptr;
+    double *mstamp = nullptr, *rstamp = nullptr;
+    int n_mslots = 0, n_rrows = 0;
+    uint32_t *mslot = nullptr, *mslot_ptr = nullptr, *mslot_ids = nullptr;
+    uint32_t *rrow = nullptr, *rrow_ptr = nullptr, *rrow_ids = nullptr;
+    unsigned long long *node_scale = nullptr;
+    Workspace ws;
+    // host copies needed to rebuild the preconditioner when the base changes
+    std::vector<uint32_t> h_rp, h_col;
+    std::vector<char> touched;
+    PcHost pc_pairs, pc_plain;
+    int pc_loaded = -1;     // which structure is on the device
+};
+
+static void plan_free(ohm_plan *p) {
+    if (!p) return;
+    cudaFree(p->rp); cudaFree(p->col); cudaFree(p->base_vals); cudaFree(p->vals64); cudaFree(p->base_b);
+    cudaFree(p->b); cudaFree(p->vals32); cudaFree(p->x_prev); cudaFree(p->x_scratch);
+    cudaFree(p->diodes); cudaFree(p->bjts); cudaFree(p->mosfets); cudaFree(p->vaf);
+    cudaFree(p->mstamp); cudaFree(p->rstamp);
+    cudaFree(p->mslot); cudaFree(p->mslot_ptr); cudaFree(p->mslot_ids);
+    cudaFree(p->rrow); cudaFree(p->rrow_ptr); cudaFree(p->rrow_ids);
+    cudaFree(p->node_scale);
+    p->ws.release();
+    delete p;
+}
+
+// Stamp map: every (slot, contribution id) pair, grouped by slot.  Ids are
+// assigned diodes first, then BJTs, then MOSFETs, device-major, so each slot
+// sums its contributions in that fixed (canonical) order.
+static void build_stamp_map(const std::vector<std::pair<uint32_t, uint32_t>> &pairs_in,
+                            std::vector<uint32_t> &slots, std::vector<uint32_t> &ptr, std::vector<uint32_t> &ids) {
+    std::vector<std::pair<uint32_t, uint32_t>> pairs(pairs_in);
+    std::stable_sort(pairs.begin(), pairs.end(),
+                     [](const auto &x, const auto &y) { return x.first < y.first; });
+    slots.clear(); ptr.clear(); ids.clear();
+    for (size_t k = 0; k < pairs.size(); ++k) {
+        if (k == 0 || pairs[k].first != pairs[k - 1].first) {
+            slots.push_back(pairs[k].first);
+            ptr.push_back((uint32_t)ids.size());
+        }
+        ids.push_back(pairs[k].second);
+    }
+    ptr.push_back((uint32_t)ids.size());
+}
+
+template <typename T>
+static cudaError_t up(T **dst, const T *src, size_t count, cudaStream_t s) {
+    cudaError_t e = dalloc(dst, count);
+    if (e == cudaSuccess && count && src) e = cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, const uint32_t *col_indices,
+                                      const uint32_t *row_ptrs, const double *base_b,
+                                      const ohm_diode_desc *diodes, int64_t n_diodes, const ohm_bjt_desc *bjts,
+                                      int64_t n_bjts, const ohm_mosfet_desc *mosfets, int64_t n_mosfets,
+                                      const double *bjt_vaf, int64_t size, int64_t nnz, ohm_plan **out) {
+    if (!c || !out) return fail(OHM_ERR_INVALID_ARG, "null ctx or out");
+    *out = nullptr;
+    if (size <= 0) return fail(OHM_ERR_INVALID_ARG, "system size must be > 0");
+    if (!base_g_values || !base_b) return fail(OHM_ERR_INVALID_ARG, "null base values / rhs");
+    ohm_status st = check_csr(size, nnz, row_ptrs, col_indices);
+    if (st != OHM_OK) return st;
+    st = check_devices(diodes, n_diodes, bjts, n_bjts, mosfets, n_mosfets, size, nnz);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaSetDevice(c->device));
+    ohm_plan *p = new (std::nothrow) ohm_plan();
+    if (!p) return fail(OHM_ERR_INVALID_ARG, "out of host memory");
+    p->ctx = c; p->n = size; p->nnz = nnz; p->nd = n_diodes; p->nq = n_bjts; p->nm = n_mosfets;
+    cudaStream_t s = c->stream;
+
+    // stamp map
+    std::vector<std::pair<uint32_t, uint32_t>> mp, rp_;
+    const uint32_t base_q = 4u * (uint32_t)n_diodes, base_m = base_q + 9u * (uint32_t)n_bjts;
+    const uint32_t rbase_q = 2u * (uint32_t)n_diodes, rbase_m = rbase_q + 3u * (uint32_t)n_bjts;
+    for (int64_t k = 0; k < n_diodes; ++k) {
+        for (int j = 0; j < 4; ++j) if (diodes[k].g_row_col[j] != kSentinel) mp.push_back({diodes[k].g_row_col[j], (uint32_t)(4 * k + j)});
+        for (int j = 0; j < 2; ++j) if (diodes[k].b_idx[j] != kSentinel) rp_.push_back({diodes[k].b_idx[j], (uint32_t)(2 * k + j)});
+    }
+    for (int64_t k = 0; k < n_bjts; ++k) {
+        for (int j = 0; j < 9; ++j) if (bjts[k].g_row_col[j] != kSentinel) mp.push_back({bjts[k].g_row_col[j], base_q + (uint32_t)(9 * k + j)});
+        for (int j = 0; j < 3; ++j) if (bjts[k].b_idx[j] != kSentinel) rp_.push_back({bjts[k].b_idx[j], rbase_q + (uint32_t)(3 * k + j)});
+    }
+    for (int64_t k = 0; k < n_mosfets; ++k) {
+        for (int j = 0; j < 6; ++j) if (mosfets[k].g_row_col[j] != kSentinel) mp.push_back({mosfets[k].g_row_col[j], base_m + (uint32_t)(6 * k + j)});
+        for (int j = 0; j < 2; ++j) if (mosfets[k].b_idx[j] != kSentinel) rp_.push_back({mosfets[k].b_idx[j], rbase_m + (uint32_t)(2 * k + j)});
+    }
+    std::vector<uint32_t> ms, mptr, mids, rs, rptr, rids;
+    build_stamp_map(mp, ms, mptr, mids);
+    build_stamp_map(rp_, rs, rptr, rids);
+    p->n_mslots = (int)ms.size();
+    p->n_rrows = (int)rs.size();
+    p->touched.assign(nnz, 0);
+    for (uint32_t sl : ms) p->touched[sl] = 1;
+    p->h_rp.assign(row_ptrs, row_ptrs + size + 1);
+    p->h_col.assign(col_indices, col_indices + nnz);
+    build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, true, p->pc_pairs);
+    build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, false, p->pc_plain);
+
+    cudaError_t e = up(&p->rp, row_ptrs, size + 1, s);
+    if (e == cudaSuccess) e = up(&p->col, col_indices, nnz, s);
+    if (e == cudaSuccess) e = up(&p->base_vals, base_g_values, nnz, s);
+    if (e == cudaSuccess) e = up(&p->vals64, base_g_values, nnz, s);
+    if (e == cudaSuccess) e = dalloc(&p->vals32, nnz);
+    if (e == cudaSuccess) e = up(&p->base_b, base_b, size, s);
+    if (e == cudaSuccess) e = up(&p->b, base_b, size, s);
+    if (e == cudaSuccess) e = dalloc(&p->x_prev, size);
+    if (e == cudaSuccess) e = dalloc(&p->x_scratch, size);
+    if (e == cudaSuccess) e = up(&p->diodes, (const DiodeDesc *)diodes, n_diodes, s);
+    if (e == cudaSuccess) e = up(&p->bjts, (const BjtDesc *)bjts, n_bjts, s);
+    if (e == cudaSuccess) e = up(&p->mosfets, (const MosfetDesc *)mosfets, n_mosfets, s);
+    if (e == cudaSuccess && bjt_vaf && n_bjts) e = up(&p->vaf, bjt_vaf, n_bjts, s);
+    if (e == cudaSuccess) e = dalloc(&p->mstamp, 4 * n_diodes + 9 * n_bjts + 6 * n_mosfets);
+    if (e == cudaSuccess) e = dalloc(&p->rstamp, 2 * n_diodes + 3 * n_bjts + 2 * n_mosfets);
+    if (e == cudaSuccess) e = up(&p->mslot, ms.data(), ms.size(), s);
+    if (e == cudaSuccess) e = up(&p->mslot_ptr, mptr.data(), mptr.size(), s);
+    if (e == cudaSuccess) e = up(&p->mslot_ids, mids.data(), mids.size(), s);
+    if (e == cudaSuccess) e = up(&p->rrow, rs.data(), rs.size(), s);
+    if (e == cudaSuccess) e = up(&p->rrow_ptr, rptr.data(), rptr.size(), s);
+    if (e == cudaSuccess) e = up(&p->rrow_ids, rids.data(), rids.size(), s);
+    if (e == cudaSuccess) e = dalloc(&p->node_scale, size);
+    if (e == cudaSuccess) e = p->ws.alloc(size, c->num_sms);
+    if (e == cudaSuccess && nnz) {
+        f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, nnz);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        plan_free(p);
+        return fail(OHM_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e));
+    }
+    *out = p;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_plan_destroy(ohm_plan *p) {
+    if (!p) return OHM_OK;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    plan_free(p);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_plan_set_base(ohm_plan *p, const double *base_g_values, const double *base_b) {
+    if (!p) return fail(OHM_ERR_INVALID_ARG, "plan is null");
+    cudaStream_t s = p->ctx->stream;
+    CUDA_TRY(cudaSetDevice(p->ctx->device));
+    if (base_g_values && p->nnz) {
+        CUDA_TRY(cudaMemcpyAsync(p->base_vals, base_g_values, p->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(p->vals64, base_g_values, p->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((p->nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, p->nnz);
+        CUDA_TRY(cudaGetLastError());
+        build_precond(p->n, p->h_rp.data(), p->h_col.data(), base_g_values, p->touched, true, p->pc_pairs);
+        p->pc_loaded = -1;
+    }
+    if (base_b) {
+        CUDA_TRY(cudaMemcpyAsync(p->base_b, base_b, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(p->b, base_b, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return OHM_OK;
+}
+
+static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, KernelArgs &a) {
+    const ohm_krylov_params &kp = np->krylov;
+    const int want_pc = kp.precond == OHM_PRECOND_AUTO ? 1 : 0;
+    if (p->pc_loaded != want_pc) {
+        cudaError_t e = p->ws.upload_pc(want_pc ? p->pc_pairs : p->pc_plain, p->ctx->stream);
+        if (e != cudaSuccess) return fail(OHM_ERR_CUDA, "preconditioner upload: %s", cudaGetErrorString(e));
+        p->pc_loaded = want_pc;
+    }
+    a = KernelArgs{};
+    a.n = (int)p->n; a.nnz = (int)p->nnz;
+    a.row_ptr = p->rp; a.col = p->col;
+    a.vals64 = p->vals64; a.vals32 = p->vals32;
+    a.base_vals = p->base_vals; a.base_b = p->base_b; a.b = p->b;
+    a.x = x_dev; a.x_prev = p->x_prev;
+    a.precond = kp.precond == OHM_PRECOND_NONE ? kPcNone : (kp.precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
+    p->ws.bind(a);
+    a.nd = (int)p->nd; a.nq = (int)p->nq; a.nm = (int)p->nm;
+    a.diodes = p->diodes; a.bjts = p->bjts; a.mosfets = p->mosfets; a.bjt_vaf = p->vaf;
+    a.mstamp = p->mstamp; a.rstamp = p->rstamp;
+    a.n_mslots = p->n_mslots; a.mslot = p->mslot; a.mslot_ptr = p->mslot_ptr; a.mslot_ids = p->mslot_ids;
+    a.n_rrows = p->n_rrows; a.rrow = p->rrow; a.rrow_ptr = p->rrow_ptr; a.rrow_ids = p->rrow_ids;
+    a.node_scale = p->node_scale;
+    a.newton = 1;
+    a.max_outer = np->max_iterations;
+    a.abs_tol = np->abs_tol;
+    a.rel_tol = np->rel_tol;
+    a.max_krylov = kp.max_iterations;
+    a.krylov_tol = kp.tolerance;
+    const bool mixed = kp.precision == OHM_PREC_MIXED;
+    a.inner_rtol = mixed ? (kp.inner_rtol > 0.0 ? kp.inner_rtol : 1e-4) : kp.inner_rtol;
+    a.accept_partial = mixed ? 1 : 0;
+    a.max_restarts = std::max(0, kp.max_restarts);
+    return OHM_OK;
+}
+
+static ohm_status check_newton(const ohm_newton_params *np) {
+    if (!np) return fail(OHM_ERR_INVALID_ARG, "params is null");
+    if (np->max_iterations <= 0)
+        return fail(OHM_ERR_NEWTON_NOT_CONVERGED, "Newton solver did not converge after 0 iterations");
+    if (!(np->abs_tol >= 0.0) || !(np->rel_tol >= 0.0)) return fail(OHM_ERR_INVALID_ARG, "negative tolerance");
+    return check_krylov(&np->krylov);
+}
+
+extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const ohm_newton_params *np,
+                                             ohm_solve_info *info) {
+    if (!p || !x_dev) return fail(OHM_ERR_INVALID_ARG, "null plan or x");
+    ohm_status st = check_newton(np);
+    if (st != OHM_OK) return st;
+    ohm_ctx *c = p->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (np->initial_guess)
+        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, p->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    KernelArgs a;
+    st = plan_args(p, np, x_dev, a);
+    if (st != OHM_OK) return st;
+    int launches = 0;
+    st = launch_solver(c, a, np->krylov.precision == OHM_PREC_MIXED, p->nnz, &launches);
+    if (st != OHM_OK) return st;
+    return finish_solver(c, info, launches);
+}
+
+extern "C" ohm_status ohm_newton_solve(ohm_ctx *c, const double *base_g_values, const uint32_t *col_indices,
+                                       const uint32_t *row_ptrs, const double *base_b, const ohm_diode_desc *diodes,
+                                       int64_t n_diodes, const ohm_bjt_desc *bjts, int64_t n_bjts,
+                                       const ohm_mosfet_desc *mosfets, int64_t n_mosfets, int64_t size, int64_t nnz,
+                                       const ohm_newton_params *params, double *x_out, ohm_solve_info *info) {
+    if (!x_out) return fail(OHM_ERR_INVALID_ARG, "x_out is null");
+    ohm_status st = check_newton(params);
+    if (st != OHM_OK) return st;
+    ohm_plan *p = nullptr;
+    st = ohm_plan_create(c, base_g_values, col_indices, row_ptrs, base_b, diodes, n_diodes, bjts, n_bjts, mosfets,
+                         n_mosfets, nullptr, size, nnz, &p);
+    if (st != OHM_OK) return st;
+    cudaError_t e = cudaMemsetAsync(p->x_scratch, 0, size * sizeof(double), c->stream);
+    if (e != cudaSuccess) { plan_free(p); return fail(OHM_ERR_CUDA, "x init: %s", cudaGetErrorString(e)); }
+    st = ohm_plan_newton_device(p, p->x_scratch, params, info);
+    // The iterate is returned on success; on NewtonNotConverged the caller
+    // still gets the last iterate (the reference downloads it, newton.rs:491-512).
+    if (st == OHM_OK || st == OHM_ERR_NEWTON_NOT_CONVERGED) {
+        e = cudaMemcpyAsync(x_out, p->x_scratch, size * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    }
+    ohm_plan_destroy(p);
+    return st;
+}
+
+extern "C" ohm_status ohm_solve_real_device(ohm_ctx *c, const ohm_csr *a, const ohm_buf *b, ohm_buf *x,
+                                            const ohm_krylov_params *params, ohm_solve_info *info) {
+    if (!c || !a || !b || !x) return fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_status st = check_krylov(params);
+    if (st != OHM_OK) return st;
+    if (b->n != a->n || x->n != a->n) return fail(OHM_ERR_INVALID_ARG, "dimension mismatch");
+    if (a->n == 0) return OHM_OK;
+    CUDA_TRY(cudaSetDevice(c->device));
+    // the preconditioner structure is built on the host from the pattern
+    std::vector<uint32_t> rp(a->n + 1), col(a->nnz);
+    std::vector<double> val(a->nnz);
+    CUDA_TRY(cudaMemcpyAsync(rp.data(), a->rp, rp.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (a->nnz) {
+        CUDA_TRY(cudaMemcpyAsync(col.data(), a->col, col.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(val.data(), a->val, val.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CUDA_TRY(cudaMemsetAsync(x->d, 0, a->n * sizeof(double), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return solve_real_impl(c, a->n, a->nnz, a->rp, a->col, a->val, rp.data(), col.data(), val.data(), b->d, x->d,
+                           params, info);
+}
+
+// ------------------------------------------- single steps (NonlinearBackend) --
+// evaluate_* + assemble_* (nonlinear.rs:31-150) as stand-alone launches, for
+// callers that drive the Newton loop themselves and for the tests.
+namespace {
+
+__global__ void eval_devices_kernel(KernelArgs a) {
+    const int ndev = a.nd + a.nq + a.nm;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ndev; k += gridDim.x * blockDim.x) {
+        if (k < a.nd) {
+            diode_stamps(a.diodes[k], a.x, a.mstamp + 4 * (size_t)k, a.rstamp + 2 * (size_t)k);
+        } else if (k < a.nd + a.nq) {
+            const int q = k - a.nd;
+            const double vaf = a.bjt_vaf ? a.bjt_vaf[q] : __longlong_as_double(0x7ff0000000000000LL);
+            bjt_stamps(a.bjts[q], vaf, a.x, a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)q,
+                       a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)q);
+        } else {
+            const int m = k - a.nd - a.nq;
+            mosfet_stamps(a.mosfets[m], a.x, a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)a.nq + 6 * (size_t)m,
+                          a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)a.nq + 2 * (size_t)m);
+        }
+    }
+}
+
+__global__ void assemble_kernel(KernelArgs a) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n_mslots + a.n_rrows; k += gridDim.x * blockDim.x) {
+        if (k < a.n_mslots) {
+            const uint32_t slot = a.mslot[k];
+            double acc = a.base_vals[slot];
+            for (uint32_t j = a.mslot_ptr[k]; j < a.mslot_ptr[k + 1]; ++j) acc += a.mstamp[a.mslot_ids[j]];
+            a.vals64[slot] = acc;
+            if (a.vals32) a.vals32[slot] = (float)acc;
+        } else {
+            const int q = k - a.n_mslots;
+            const uint32_t row = a.rrow[q];
+            double acc = a.base_b[row];
+            for (uint32_t j = a.rrow_ptr[q]; j < a.rrow_ptr[q + 1]; ++j) acc += a.rstamp[a.rrow_ids[j]];
+            a.b[row] = acc;
+        }
+    }
+}
+
+__global__ void limit_reset_kernel(int n, unsigned long long *scale) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        scale[i] = 0x3FF0000000000000ULL;
+}
+
+__global__ void limit_propose_kernel(KernelArgs a) {
+    const int ndev = a.nd + a.nq + a.nm;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ndev; k += gridDim.x * blockDim.x) {
+        if (k < a.nd) diode_limit(a.diodes[k], a.x_prev, a.x, a.node_scale);
+        else if (k < a.nd + a.nq) bjt_limit(a.bjts[k - a.nd], a.x_prev, a.x, a.node_scale);
+        else mosfet_limit(a.mosfets[k - a.nd - a.nq], a.x_prev, a.x, a.node_scale);
+    }
+}
+
+__global__ void limit_apply_kernel(int n, const double *xo, double *xn, const unsigned long long *scale) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double sc = __longlong_as_double((long long)scale[i]);
+        if (sc < 1.0) xn[i] = xo[i] + (xn[i] - xo[i]) * sc;
+    }
+}
+
+int steps_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+
+}  // namespace
+
+extern "C" ohm_status ohm_plan_assemble(ohm_plan *p, const double *x_host, double *values_out, double *rhs_out) {
+    if (!p || !x_host) return fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_ctx *c = p->ctx;
+    cudaStream_t s = c->stream;
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaMemcpyAsync(p->x_scratch, x_host, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    ohm_newton_params np;
+    ohm_newton_params_default(&np);
+    KernelArgs a;
+    ohm_status st = plan_args(p, &np, p->x_scratch, a);
+    if (st != OHM_OK) return st;
+    const int64_t ndev = p->nd + p->nq + p->nm;
+    if (ndev) eval_devices_kernel<<<steps_grid(ndev), 256, 0, s>>>(a);
+    if (p->n_mslots + p->n_rrows) assemble_kernel<<<steps_grid(p->n_mslots + p->n_rrows), 256, 0, s>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return ohm_plan_download_system(p, values_out, rhs_out);
+}
+
+extern "C" ohm_status ohm_plan_download_system(ohm_plan *p, double *values, double *rhs) {
+    if (!p) return fail(OHM_ERR_INVALID_ARG, "plan is null");
+    cudaStream_t s = p->ctx->stream;
+    if (values && p->nnz) CUDA_TRY(cudaMemcpyAsync(values, p->vals64, p->nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (rhs) CUDA_TRY(cudaMemcpyAsync(rhs, p->b, p->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_plan_limit(ohm_plan *p, const double *x_old_host, double *x_new_inout) {
+    if (!p || !x_old_host || !x_new_inout) return fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_ctx *c = p->ctx;
+    cudaStream_t s = c->stream;
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaMemcpyAsync(p->x_prev, x_old_host, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(p->x_scratch, x_new_inout, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    ohm_newton_params np;
+    ohm_newton_params_default(&np);
+    KernelArgs a;
+    ohm_status st = plan_args(p, &np, p->x_scratch, a);
+    if (st != OHM_OK) return st;
+    limit_reset_kernel<<<steps_grid(p->n), 256, 0, s>>>((int)p->n, p->node_scale);
+    const int64_t ndev = p->nd + p->nq + p->nm;
+    if (ndev) limit_propose_kernel<<<steps_grid(ndev), 256, 0, s>>>(a);
+    limit_apply_kernel<<<steps_grid(p->n), 256, 0, s>>>((int)p->n, p->x_prev, p->x_scratch, p->node_scale);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(x_new_inout, p->x_scratch, p->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return OHM_OK;
+}

@@ -1,0 +1,56 @@
+// Internal declarations shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <string>
+
+#include "../../include/ohm.h"
+#include "solver_kernel.cuh"
+
+using ohm::DeviceInfo;
+
+// Records the message for ohm_last_error() and returns `st`.
+ohm_status ohm_fail(ohm_status st, const char *fmt, ...);
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return ohm_fail(OHM_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));  \
+    } while (0)
+
+// ---------------------------------------------------------------- context --
+struct ohm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    // barrier words + info block
+    unsigned int *sync_words = nullptr;   // [count, gen, error(int)]
+    DeviceInfo *info_dev = nullptr;
+    DeviceInfo *info_host = nullptr;      // pinned
+    double *dot_scratch = nullptr;        // for ohm_dot
+};
+
+struct ohm_buf {
+    ohm_ctx *ctx;
+    double *d;
+    int64_t n;
+};
+
+struct ohm_csr {
+    ohm_ctx *ctx;
+    int64_t n, nnz;
+    uint32_t *rp, *col;
+    double *val;
+};
+
+template <typename T>
+inline cudaError_t dalloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void **)p, count * sizeof(T));
+}
+

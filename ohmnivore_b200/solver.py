@@ -1,0 +1,419 @@
+"""Host-side mirror of the reference's solver interfaces over the C ABI.
+
+  ``LinearSolver`` / ``GpuSolver.solve_real``   src/solver/mod.rs:27-34, gpu.rs:107-208
+  ``SolverBackend`` (buffers, spmv, dot, ...)   src/solver/backend.rs:51-96
+  ``BiCgStabParams``                            src/solver/bicgstab.rs:14-27
+  ``NewtonParams``, ``newton_solve``            src/solver/newton.rs:34-78
+  error taxonomy                                src/error.rs:4-33
+
+Every call goes through ``libohm_b200.so``; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import dptr, u32ptr, vptr
+
+DEFAULT_MAX_ITERATIONS = 10_000   # bicgstab.rs:10
+DEFAULT_TOLERANCE = 1e-5          # bicgstab.rs:11
+
+
+class OhmnivoreError(RuntimeError):
+    """Base of the error taxonomy (src/error.rs:4-33)."""
+
+
+class CompileError(OhmnivoreError):
+    pass
+
+
+class SolveError(OhmnivoreError):
+    def __init__(self, msg, krylov_code=None):
+        super().__init__(msg)
+        self.krylov_code = krylov_code
+
+
+class NewtonNotConverged(OhmnivoreError):
+    def __init__(self, msg, iterations, max_residual, x=None):
+        super().__init__(msg)
+        self.iterations = iterations
+        self.max_residual = max_residual
+        self.x = x
+
+
+class NewtonNumericalError(OhmnivoreError):
+    def __init__(self, msg, iteration):
+        super().__init__(msg)
+        self.iteration = iteration
+
+
+class DeviceTimeout(OhmnivoreError):
+    pass
+
+
+class InvalidArgument(OhmnivoreError, ValueError):
+    pass
+
+
+def _raise(st, info=None, x=None):
+    msg = _lib.last_error()
+    if st == _lib.ERR_SOLVE:
+        raise SolveError(msg, None if info is None else info.krylov_code)
+    if st == _lib.ERR_NEWTON_NOT_CONVERGED:
+        raise NewtonNotConverged(msg, 0 if info is None else info.iterations,
+                                 0.0 if info is None else info.max_residual, x)
+    if st == _lib.ERR_NEWTON_NUMERICAL:
+        raise NewtonNumericalError(msg, 0 if info is None else info.error_iteration)
+    if st == _lib.ERR_COMPILE:
+        raise CompileError(msg)
+    if st == _lib.ERR_TIMEOUT:
+        raise DeviceTimeout(msg)
+    if st == _lib.ERR_INVALID_ARG:
+        raise InvalidArgument(msg)
+    raise OhmnivoreError(f"status {st}: {msg}")
+
+
+@dataclass
+class BiCgStabParams:
+    """``BiCgStabParams`` (bicgstab.rs:14-27) plus the B200 extensions."""
+    max_iterations: int = DEFAULT_MAX_ITERATIONS
+    tolerance: float = DEFAULT_TOLERANCE
+    precision: int = _lib.PREC_FP64
+    precond: int = _lib.PRECOND_AUTO
+    inner_rtol: float = 0.0
+    max_refinements: int = 1
+    max_restarts: int = 50
+
+    def to_c(self) -> _lib.KrylovParams:
+        p = _lib.KrylovParams()
+        _lib.load().ohm_krylov_params_default(C.byref(p))
+        p.max_iterations = int(self.max_iterations)
+        p.tolerance = float(self.tolerance)
+        p.precision = int(self.precision)
+        p.precond = int(self.precond)
+        p.inner_rtol = float(self.inner_rtol)
+        p.max_refinements = int(self.max_refinements)
+        p.max_restarts = int(self.max_restarts)
+        return p
+
+
+@dataclass
+class NewtonParams:
+    """``NewtonParams`` (newton.rs:34-55) plus extensions (rel_tol, precision)."""
+    max_iterations: int = 50
+    abs_tol: float = 1e-4
+    bicgstab_max_iterations: int = DEFAULT_MAX_ITERATIONS
+    initial_guess: np.ndarray | None = None
+    rel_tol: float = 0.0
+    bicgstab_tolerance: float = DEFAULT_TOLERANCE
+    precision: int = _lib.PREC_FP64
+    precond: int = _lib.PRECOND_AUTO
+    inner_rtol: float = 0.0
+
+    def to_c(self):
+        p = _lib.NewtonParamsC()
+        _lib.load().ohm_newton_params_default(C.byref(p))
+        p.max_iterations = int(self.max_iterations)
+        p.abs_tol = float(self.abs_tol)
+        p.rel_tol = float(self.rel_tol)
+        p.krylov = BiCgStabParams(self.bicgstab_max_iterations, self.bicgstab_tolerance,
+                                  self.precision, self.precond, self.inner_rtol).to_c()
+        keep = None
+        if self.initial_guess is not None:
+            keep = np.ascontiguousarray(self.initial_guess, dtype=np.float64)
+            p.initial_guess = dptr(keep)
+        return p, keep
+
+
+class Context:
+    """One CUDA device + stream (``WgpuDsBackend::new``)."""
+
+    def __init__(self, device: int = 0):
+        lib = _lib.load()
+        h = C.c_void_p()
+        st = lib.ohm_ctx_create(int(device), C.byref(h))
+        if st != _lib.OK:
+            _raise(st)
+        self._h = h
+        self.lib = lib
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        st = self.lib.ohm_ctx_synchronize(self._h)
+        if st:
+            _raise(st)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.ohm_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_DEFAULT_CTX = None
+
+
+def default_context() -> Context:
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+def _csr_u32(a):
+    rp = np.ascontiguousarray(a.row_ptr, dtype=np.uint32)
+    ci = np.ascontiguousarray(a.col, dtype=np.uint32)
+    return rp, ci
+
+
+class GpuSolver:
+    """``LinearSolver`` implementation (src/solver/gpu.rs:107-208)."""
+
+    def __init__(self, ctx: Context | None = None, params: BiCgStabParams | None = None):
+        self.ctx = ctx or default_context()
+        self.params = params or BiCgStabParams()
+        self.last_info = None
+
+    def solve_real(self, a, b, params: BiCgStabParams | None = None) -> np.ndarray:
+        n = int(a.nrows)
+        if a.ncols != n or len(b) != n:
+            raise SolveError(f"dimension mismatch: matrix is {a.nrows}x{a.ncols}, rhs length is {len(b)}")
+        if n == 0:
+            return np.zeros(0)
+        rp, ci = _csr_u32(a)
+        val = np.ascontiguousarray(a.val, dtype=np.float64)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(n)
+        info = _lib.SolveInfo()
+        p = (params or self.params).to_c()
+        st = self.ctx.lib.ohm_solve_real(self.ctx.handle, n, len(ci), u32ptr(rp), u32ptr(ci), dptr(val),
+                                         dptr(bb), dptr(x), C.byref(p), C.byref(info))
+        self.last_info = info.as_dict()
+        if st != _lib.OK:
+            _raise(st, info)
+        return x
+
+
+def newton_solve(ctx, base_g_values, col_indices, row_ptrs, base_b, diode_descriptors,
+                 bjt_descriptors, mosfet_descriptors, system_size, matrix_nnz,
+                 params: NewtonParams | None = None, stats: dict | None = None) -> np.ndarray:
+    """``newton_solve`` (src/solver/newton.rs:65-78), same argument order.
+
+    Descriptor arrays are numpy structured arrays with the reference byte
+    layout (``ohmnivore_b200.mna.DIODE_DTYPE`` etc.).  Returns x (FP64).
+    """
+    ctx = ctx or default_context()
+    params = params or NewtonParams()
+    vals = np.ascontiguousarray(base_g_values, dtype=np.float64)
+    ci = np.ascontiguousarray(col_indices, dtype=np.uint32)
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.uint32)
+    bb = np.ascontiguousarray(base_b, dtype=np.float64)
+    dd = np.ascontiguousarray(diode_descriptors)
+    qd = np.ascontiguousarray(bjt_descriptors)
+    md = np.ascontiguousarray(mosfet_descriptors)
+    x = np.zeros(int(system_size))
+    info = _lib.SolveInfo()
+    p, keep = params.to_c()
+    st = ctx.lib.ohm_newton_solve(ctx.handle, dptr(vals), u32ptr(ci), u32ptr(rp), dptr(bb),
+                                  vptr(dd), len(dd), vptr(qd), len(qd), vptr(md), len(md),
+                                  int(system_size), int(matrix_nnz), C.byref(p), dptr(x),
+                                  C.byref(info))
+    del keep
+    if stats is not None:
+        stats.update(info.as_dict())
+    if st != _lib.OK:
+        _raise(st, info, x)
+    return x
+
+
+class NewtonPlan:
+    """Device-resident nonlinear system: uploads once, solves many times."""
+
+    def __init__(self, sysm, ctx: Context | None = None, base_vals=None, base_b=None):
+        self.ctx = ctx or default_context()
+        self.sysm = sysm
+        self.n = int(sysm.size)
+        self.nnz = int(sysm.g.nnz)
+        vals = np.ascontiguousarray(sysm.g.val if base_vals is None else base_vals, dtype=np.float64)
+        rp, ci = _csr_u32(sysm.g)
+        bb = np.ascontiguousarray(sysm.b_dc if base_b is None else base_b, dtype=np.float64)
+        dd = np.ascontiguousarray(sysm.diode_descriptors)
+        qd = np.ascontiguousarray(sysm.bjt_descriptors)
+        md = np.ascontiguousarray(sysm.mosfet_descriptors)
+        vaf = None
+        if len(qd) and sysm.bjt_vaf is not None and np.any(np.isfinite(sysm.bjt_vaf)):
+            vaf = np.ascontiguousarray(sysm.bjt_vaf, dtype=np.float64)
+        h = C.c_void_p()
+        st = self.ctx.lib.ohm_plan_create(self.ctx.handle, dptr(vals), u32ptr(ci), u32ptr(rp), dptr(bb),
+                                          vptr(dd), len(dd), vptr(qd), len(qd), vptr(md), len(md),
+                                          None if vaf is None else dptr(vaf), self.n, self.nnz,
+                                          C.byref(h))
+        if st != _lib.OK:
+            _raise(st)
+        self._h = h
+        self.last_info = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.ohm_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_base(self, base_vals=None, base_b=None):
+        v = None if base_vals is None else np.ascontiguousarray(base_vals, dtype=np.float64)
+        b = None if base_b is None else np.ascontiguousarray(base_b, dtype=np.float64)
+        st = self.ctx.lib.ohm_plan_set_base(self._h, None if v is None else dptr(v),
+                                            None if b is None else dptr(b))
+        if st:
+            _raise(st)
+
+    def newton_device(self, x_dev_ptr: int, params: NewtonParams | None = None) -> dict:
+        """Run Newton on a device vector (raw CUDA pointer, e.g. torch ``data_ptr()``)."""
+        p, keep = (params or NewtonParams()).to_c()
+        info = _lib.SolveInfo()
+        st = self.ctx.lib.ohm_plan_newton_device(self._h, C.c_void_p(int(x_dev_ptr)), C.byref(p),
+                                                 C.byref(info))
+        del keep
+        self.last_info = info.as_dict()
+        if st != _lib.OK:
+            _raise(st, info)
+        return self.last_info
+
+    def assemble(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        vals = np.zeros(self.nnz)
+        rhs = np.zeros(self.n)
+        st = self.ctx.lib.ohm_plan_assemble(self._h, dptr(x), dptr(vals), dptr(rhs))
+        if st:
+            _raise(st)
+        return vals, rhs
+
+    def limit(self, x_old, x_new):
+        xo = np.ascontiguousarray(x_old, dtype=np.float64)
+        xn = np.array(x_new, dtype=np.float64, copy=True)
+        st = self.ctx.lib.ohm_plan_limit(self._h, dptr(xo), dptr(xn))
+        if st:
+            _raise(st)
+        return xn
+
+
+class DeviceBuffer:
+    """``SolverBackend::Buffer``: FP64 device vector."""
+
+    def __init__(self, ctx: Context, n: int):
+        self.ctx, self.n = ctx, int(n)
+        h = C.c_void_p()
+        st = ctx.lib.ohm_buf_create(ctx.handle, self.n, C.byref(h))
+        if st:
+            _raise(st)
+        self._h = h
+
+    def upload(self, host):
+        a = np.ascontiguousarray(host, dtype=np.float64)
+        st = self.ctx.lib.ohm_buf_upload(self.ctx.handle, self._h, dptr(a), len(a))
+        if st:
+            _raise(st)
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        st = self.ctx.lib.ohm_buf_download(self.ctx.handle, self._h, dptr(out), self.n)
+        if st:
+            _raise(st)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.ohm_buf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceCsr:
+    """``GpuCsrMatrix``."""
+
+    def __init__(self, ctx: Context, a):
+        self.ctx, self.n, self.nnz = ctx, int(a.nrows), int(a.nnz)
+        rp, ci = _csr_u32(a)
+        val = np.ascontiguousarray(a.val, dtype=np.float64)
+        h = C.c_void_p()
+        st = ctx.lib.ohm_csr_upload(ctx.handle, self.n, self.nnz, u32ptr(rp), u32ptr(ci), dptr(val),
+                                    C.byref(h))
+        if st:
+            _raise(st)
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.ohm_csr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolverBackend:
+    """``SolverBackend`` trait operations (backend.rs:51-96) on device buffers."""
+
+    def __init__(self, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+
+    def new_buffer(self, n):
+        return DeviceBuffer(self.ctx, n)
+
+    def upload_matrix(self, a):
+        return DeviceCsr(self.ctx, a)
+
+    def _chk(self, st):
+        if st:
+            _raise(st)
+
+    def spmv(self, a: DeviceCsr, x: DeviceBuffer, y: DeviceBuffer):
+        self._chk(self.ctx.lib.ohm_spmv(self.ctx.handle, a._h, x._h, y._h))
+
+    def dot(self, a: DeviceBuffer, b: DeviceBuffer) -> float:
+        out = C.c_double()
+        self._chk(self.ctx.lib.ohm_dot(self.ctx.handle, a._h, b._h, C.byref(out)))
+        return out.value
+
+    def axpy(self, alpha, x, y):
+        self._chk(self.ctx.lib.ohm_axpy(self.ctx.handle, float(alpha), x._h, y._h))
+
+    def copy(self, src, dst):
+        self._chk(self.ctx.lib.ohm_copy(self.ctx.handle, src._h, dst._h))
+
+    def scale(self, alpha, x):
+        self._chk(self.ctx.lib.ohm_scale(self.ctx.handle, float(alpha), x._h))
+
+    def solve_real_device(self, a: DeviceCsr, b: DeviceBuffer, x: DeviceBuffer,
+                          params: BiCgStabParams | None = None) -> dict:
+        p = (params or BiCgStabParams()).to_c()
+        info = _lib.SolveInfo()
+        st = self.ctx.lib.ohm_solve_real_device(self.ctx.handle, a._h, b._h, x._h, C.byref(p),
+                                                C.byref(info))
+        if st:
+            _raise(st, info)
+        return info.as_dict()

@@ -1,0 +1,147 @@
+"""GPU parity: linear solves and SolverBackend ops through the C ABI vs the oracle."""
+import numpy as np
+import pytest
+
+from oracle import linear_ref
+from oracle.mna_ref import RefCsr
+from ohmnivore_b200 import circuits as ck
+from ohmnivore_b200 import mna
+from ohmnivore_b200 import solver as S
+from tests.golden import known_answers as KA
+
+pytestmark = pytest.mark.gpu
+
+
+def _mcsr(case):
+    a = RefCsr.from_triplets(case["n"], case.get("ncols", case["n"]), case["trip"])
+    return mna.Csr(a.nrows, a.ncols, np.array(a.row_pointers, np.int64), np.array(a.col_indices, np.int64),
+                   np.array(a.values, np.float64))
+
+
+@pytest.mark.parametrize("case", KA.REAL_SOLVES, ids=lambda c: c["name"])
+def test_solve_real_known_answers(ctx, case):
+    a = _mcsr(case)
+    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-14))
+    x = solver.solve_real(a, case["b"])
+    ax = linear_ref.spmv(a.nrows, a.row_ptr, a.col, a.val, x)
+    np.testing.assert_allclose(ax, case["b"], atol=1e-10, rtol=0)
+    if case["x"] is not None:
+        np.testing.assert_allclose(x, case["x"], atol=1e-10, rtol=0)
+
+
+def test_solve_real_dimension_mismatch(ctx):
+    case = KA.REAL_ERRORS[1]
+    with pytest.raises(S.SolveError, match="dimension"):
+        S.GpuSolver(ctx).solve_real(_mcsr(case), case["b"])
+
+
+def test_solve_real_empty(ctx):
+    a = mna.Csr(0, 0, np.zeros(1, np.int64), np.zeros(0, np.int64), np.zeros(0))
+    assert S.GpuSolver(ctx).solve_real(a, []).shape == (0,)
+
+
+def test_solve_real_zero_rhs(ctx):
+    """bicgstab.rs:91-95: b = 0 -> x = 0."""
+    case = KA.REAL_SOLVES[1]
+    x = S.GpuSolver(ctx).solve_real(_mcsr(case), [0.0, 0.0])
+    np.testing.assert_array_equal(x, [0.0, 0.0])
+
+
+def test_solve_real_bad_params(ctx):
+    case = KA.REAL_SOLVES[1]
+    with pytest.raises(S.SolveError, match="max_iterations"):
+        S.GpuSolver(ctx, S.BiCgStabParams(max_iterations=0)).solve_real(_mcsr(case), case["b"])
+    with pytest.raises(S.SolveError, match="tolerance"):
+        S.GpuSolver(ctx, S.BiCgStabParams(tolerance=0.0)).solve_real(_mcsr(case), case["b"])
+
+
+def test_solve_real_maxiter_reported(ctx):
+    s = mna.compile_circuit(ck.resistor_ladder(2000, seed=5))
+    with pytest.raises(S.SolveError, match="did not converge") as ei:
+        S.GpuSolver(ctx, S.BiCgStabParams(max_iterations=1, tolerance=1e-14)).solve_real(s.g, s.b_dc)
+    assert ei.value.krylov_code == 2
+
+
+def test_solve_real_nan_rhs(ctx):
+    case = KA.REAL_SOLVES[1]
+    with pytest.raises(S.SolveError):
+        S.GpuSolver(ctx).solve_real(_mcsr(case), [np.nan, 1.0])
+
+
+@pytest.mark.parametrize("case", KA.DC_CASES, ids=lambda c: c["name"])
+def test_dc_known_answers_gpu(ctx, case):
+    """integration_test.rs:48-125 through the GPU BiCGSTAB."""
+    ckt = KA.build_circuit(case["comps"])
+    s = mna.compile_circuit(ckt)
+    x = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-13)).solve_real(s.g, s.b_dc)
+    for lbl, v in case["v"].items():
+        assert abs(x[s.node_index(lbl)] - v) < case["v_tol"]
+    for name, i in case.get("i", {}).items():
+        k = [ckt.names[c] for c in s.branch_components].index(name)
+        assert abs(x[s.n_nodes + k] - i) < case["i_tol"]
+
+
+def _rel_err(x, ref, sl):
+    return float(np.max(np.abs(x[sl] - ref[sl])) / np.max(np.abs(ref[sl])))
+
+
+@pytest.mark.parametrize("n_nodes", [200, 2000])
+def test_ladder_fp64_vs_dense_oracle(ctx, n_nodes):
+    """Resistor ladder (the 10k-node benchmark recipe, smaller): Jacobi
+    BiCGSTAB at tol 1e-12 vs the dense GE restatement, 1e-9 norm-wise."""
+    s = mna.compile_circuit(ck.resistor_ladder(n_nodes, seed=0))
+    ref = linear_ref.dense_solve_real(s.size, s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
+    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-12))
+    x = solver.solve_real(s.g, s.b_dc)
+    assert _rel_err(x, ref, slice(0, s.n_nodes)) < 1e-9
+    assert _rel_err(x, ref, slice(s.n_nodes, s.size)) < 1e-9
+
+
+@pytest.mark.slow
+def test_ladder_10k_fp64_and_mixed(ctx):
+    s = mna.compile_circuit(ck.resistor_ladder(10_000, seed=0))
+    ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
+    for prec in (0, 1):
+        p = S.BiCgStabParams(tolerance=1e-12, precision=prec, max_refinements=30, max_iterations=20000)
+        x = S.GpuSolver(ctx, p).solve_real(s.g, s.b_dc)
+        assert _rel_err(x, ref, slice(0, s.n_nodes)) < 1e-9, prec
+        assert _rel_err(x, ref, slice(s.n_nodes, s.size)) < 1e-9, prec
+
+
+def test_mixed_precision_iterative_refinement(ctx):
+    s = mna.compile_circuit(ck.diode_mesh(30, 30, seed=11, diode_frac=0.0))
+    ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
+    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-12, precision=1, max_refinements=20))
+    x = solver.solve_real(s.g, s.b_dc)
+    assert _rel_err(x, ref, slice(0, s.size)) < 1e-9
+    assert solver.last_info["iterations"] >= 2        # refinement sweeps were used
+
+
+def test_backend_ops(ctx):
+    """SolverBackend ops (backend.rs:51-96) vs numpy."""
+    s = mna.compile_circuit(ck.diode_mesh(20, 20, seed=3))
+    be = S.SolverBackend(ctx)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(s.size)
+    y0 = rng.standard_normal(s.size)
+    A = be.upload_matrix(s.g)
+    bx, by = be.new_buffer(s.size), be.new_buffer(s.size)
+    bx.upload(x)
+    be.spmv(A, bx, by)
+    np.testing.assert_allclose(by.download(), linear_ref.spmv(s.size, s.g.row_ptr, s.g.col, s.g.val, x),
+                               rtol=1e-13, atol=1e-13)
+    by.upload(y0)
+    assert abs(be.dot(bx, by) - float(x @ y0)) < 1e-12 * abs(x).sum() * abs(y0).max()
+    be.axpy(2.5, bx, by)
+    np.testing.assert_allclose(by.download(), y0 + 2.5 * x, rtol=0, atol=1e-15)
+    be.scale(-3.0, by)
+    np.testing.assert_allclose(by.download(), (y0 + 2.5 * x) * -3.0, rtol=0, atol=1e-14)
+    be.copy(bx, by)
+    np.testing.assert_array_equal(by.download(), x)
+    bsol = be.new_buffer(s.size)
+    bb = be.new_buffer(s.size)
+    bb.upload(s.b_dc)
+    info = be.solve_real_device(A, bb, bsol, S.BiCgStabParams(tolerance=1e-13))
+    ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
+    assert _rel_err(bsol.download(), ref, slice(0, s.size)) < 1e-9
+    assert info["kernel_launches"] >= 1

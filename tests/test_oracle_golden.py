@@ -1,0 +1,227 @@
+"""Pin the oracle and the host compiler against the reference's own known answers."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import devices_ref, linear_ref, mna_ref
+from oracle.mna_ref import RefCsr
+from ohmnivore_b200 import mna
+from tests.golden import known_answers as KA
+
+
+def _csr(case):
+    c = RefCsr.from_triplets(case["n"], case.get("ncols", case["n"]), case["trip"])
+    return c
+
+
+@pytest.mark.parametrize("case", KA.REAL_SOLVES, ids=lambda c: c["name"])
+def test_dense_ge_known_answers(case):
+    a = _csr(case)
+    x = linear_ref.dense_solve_real(a.nrows, a.ncols, a.row_pointers, a.col_indices, a.values, case["b"])
+    if case["x"] is not None:
+        np.testing.assert_allclose(x, case["x"], atol=case["tol"], rtol=0)
+    else:  # verified through spmv (cpu.rs:368-396)
+        ax = linear_ref.spmv(a.nrows, a.row_pointers, a.col_indices, a.values, x)
+        np.testing.assert_allclose(ax, case["b"], atol=case["tol"], rtol=0)
+
+
+@pytest.mark.parametrize("case", KA.REAL_SOLVES, ids=lambda c: c["name"])
+def test_sparse_lu_known_answers(case):
+    a = _csr(case)
+    x = linear_ref.sparse_lu_solve(a.nrows, a.row_pointers, a.col_indices, a.values, case["b"])
+    ax = linear_ref.spmv(a.nrows, a.row_pointers, a.col_indices, a.values, x)
+    np.testing.assert_allclose(ax, case["b"], atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("case", KA.REAL_ERRORS, ids=lambda c: c["name"])
+def test_dense_ge_errors(case):
+    a = _csr(case)
+    with pytest.raises(linear_ref.SolveError, match=case["err"]):
+        linear_ref.dense_solve_real(a.nrows, a.ncols, a.row_pointers, a.col_indices, a.values, case["b"])
+
+
+def test_dense_ge_empty():
+    assert linear_ref.dense_solve_real(0, 0, [0], [], [], []).shape == (0,)
+
+
+@pytest.mark.parametrize("case", KA.COMPLEX_SOLVES, ids=lambda c: c["name"])
+def test_dense_ge_complex_known_answers(case):
+    a = RefCsr.from_triplets(case["n"], case["n"], case["trip"])
+    x = linear_ref.dense_solve_complex(a.nrows, a.ncols, a.row_pointers, a.col_indices, a.values, case["b"])
+    np.testing.assert_allclose(x, case["x"], atol=case["tol"], rtol=0)
+
+
+@pytest.mark.parametrize("case", KA.COMPLEX_ERRORS, ids=lambda c: c["name"])
+def test_dense_ge_complex_errors(case):
+    a = RefCsr.from_triplets(case["n"], case["n"], case["trip"])
+    with pytest.raises(linear_ref.SolveError):
+        linear_ref.dense_solve_complex(a.nrows, a.ncols, a.row_pointers, a.col_indices, a.values, case["b"])
+
+
+@pytest.mark.parametrize("case", KA.CSR_CASES, ids=lambda c: c["name"])
+def test_from_triplets(case):
+    a = RefCsr.from_triplets(case["n"], case["n"], case["trip"])
+    assert len(a.values) == case["nnz"]
+    np.testing.assert_array_equal(a.to_dense(), case["dense"])
+    if "row_ptr" in case:
+        assert a.row_pointers == case["row_ptr"]
+
+
+@pytest.mark.parametrize("case", KA.SPMV_CASES, ids=lambda c: c["name"])
+def test_spmv(case):
+    a = RefCsr.from_triplets(case["n"], case["n"], case["trip"])
+    y = linear_ref.spmv(a.nrows, a.row_pointers, a.col_indices, a.values, case["x"])
+    np.testing.assert_array_equal(y, case["y"])
+
+
+def _check_mna(case, got, oracle):
+    if case["size"] == 0:
+        assert got.size == 0 and oracle["size"] == 0
+        return
+    gd = got.g.to_dense()
+    od = oracle["g"].to_dense()
+    for (r, c), v in case.get("g", {}).items():
+        assert abs(gd[r, c] - v) < 1e-9, (r, c, gd[r, c], v)
+        assert abs(od[r, c] - v) < 1e-9
+    for (r, c), v in case.get("c", {}).items():
+        assert abs(got.c.to_dense()[r, c] - v) < case.get("c_tol", 1e-9)
+    if "b_dc" in case:
+        np.testing.assert_allclose(got.b_dc, case["b_dc"], atol=1e-9)
+        np.testing.assert_allclose(oracle["b_dc"], case["b_dc"], atol=1e-9)
+    for k, v in case.get("b_ac", {}).items():
+        assert abs(got.b_ac[k] - v) < 1e-9
+        assert abs(oracle["b_ac"][k] - v) < 1e-9
+    assert got.size == case["size"] == oracle["size"]
+    if "node_labels" in case:
+        assert list(got.node_labels) == case["node_labels"] == list(oracle["node_labels"])
+
+
+@pytest.mark.parametrize("case", KA.MNA_CASES, ids=lambda c: c["name"])
+def test_mna_known_answers(case):
+    ckt = KA.build_circuit(case["comps"])
+    got = mna.compile_circuit(ckt)
+    oracle = mna_ref.compile_ref(ckt)
+    _check_mna(case, got, oracle)
+
+
+def test_zero_resistance_rejected():
+    """compiler.rs:1114-1123."""
+    ckt = KA.build_circuit([("R", "R1", (1, 0), 0.0)])
+    with pytest.raises(mna.CompileError, match="zero resistance"):
+        mna.compile_circuit(ckt)
+    with pytest.raises(ValueError):
+        mna_ref.compile_ref(ckt)
+
+
+def _sent(v):
+    return mna.SENTINEL if v == "S" else v
+
+
+@pytest.mark.parametrize("case", KA.DESCRIPTOR_CASES, ids=lambda c: c["name"])
+def test_descriptor_known_answers(case):
+    ckt = KA.build_circuit(case["comps"])
+    got = mna.compile_circuit(ckt)
+    ref = mna_ref.compile_ref(ckt)
+    if "diode" in case:
+        e = case["diode"]
+        d = got.diode_descriptors[0]
+        r = ref["diodes"][0]
+        assert d["anode"] == _sent(e["anode"]) == r["anode"]
+        assert d["cathode"] == _sent(e["cathode"]) == r["cathode"]
+        assert [x != mna.SENTINEL for x in d["g_row_col"]] == e["g_valid"]
+        assert list(d["g_row_col"]) == r["g_row_col"]
+        assert list(d["b_idx"]) == [_sent(v) for v in e["b_idx"]] == r["b_idx"]
+        if "is_val" in e:
+            assert abs(d["is_val"] - np.float32(e["is_val"])) < 1e-20
+            assert abs(d["n_vt"] - np.float32(e["n_vt"])) < 1e-6
+        if "g_at_aa" in case:
+            assert abs(got.g.val[d["g_row_col"][0]] - case["g_at_aa"]) < 1e-9
+    if "bjt" in case:
+        e = case["bjt"]
+        d = got.bjt_descriptors[0]
+        r = ref["bjts"][0]
+        for k in ("collector", "base", "emitter"):
+            assert d[k] == _sent(e[k]) == r[k]
+        assert [x != mna.SENTINEL for x in d["g_row_col"]] == e["g_valid"]
+        assert list(d["g_row_col"]) == r["g_row_col"]
+        assert list(d["b_idx"]) == [_sent(v) for v in e["b_idx"]] == r["b_idx"]
+        assert list(d["node_fixed"]) == r["node_fixed"]
+        for k in ("bf", "br", "nf_vt", "nr_vt", "is_val", "polarity"):
+            if k in e:
+                assert abs(float(d[k]) - e[k]) < 1e-6 * max(1.0, abs(e[k]))
+    if "mosfet" in case:
+        e = case["mosfet"]
+        d = got.mosfet_descriptors[0]
+        r = ref["mosfets"][0]
+        for k in ("drain", "gate", "source"):
+            assert d[k] == _sent(e[k]) == r[k]
+        assert [x != mna.SENTINEL for x in d["g_row_col"]] == e["g_valid"]
+        assert list(d["g_row_col"]) == r["g_row_col"]
+        assert list(d["b_idx"]) == [_sent(v) for v in e["b_idx"]] == r["b_idx"]
+        assert d["node_fixed_packed"] == r["node_fixed_packed"]
+        for k in ("vto", "kp", "lam", "polarity"):
+            if k in e:
+                assert abs(float(d[k]) - e[k]) < 1e-6 * max(1.0, abs(e[k]))
+    if "counts" in case:
+        k = case["counts"]
+        assert len(got.diode_descriptors) == k["diodes"]
+        assert len(got.bjt_descriptors) == k["bjts"]
+        assert len(got.mosfet_descriptors) == k["mosfets"]
+        assert got.n_nodes == k["n_nodes"] and got.size == k["size"]
+
+
+@pytest.mark.parametrize("case", KA.DC_CASES, ids=lambda c: c["name"])
+def test_dc_known_answers_oracle(case):
+    """integration_test.rs:48-125 through the oracle's compile + dense GE."""
+    ckt = KA.build_circuit(case["comps"])
+    s = mna.compile_circuit(ckt)
+    x = linear_ref.dense_solve_real(s.size, s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
+    for lbl, v in case["v"].items():
+        assert abs(x[s.node_index(lbl)] - v) < case["v_tol"]
+    for name, i in case.get("i", {}).items():
+        k = [ckt.names[c] for c in s.branch_components].index(name)
+        assert abs(x[s.n_nodes + k] - i) < case["i_tol"]
+
+
+def test_mosfet_model_reference_properties():
+    """Properties the reference checks on its MOSFET twin formula
+    (gpu_shaders.rs:1496-1660): cutoff current ~0, saturation current
+    KP/2 * Vov^2 (1 + lambda Vds), continuity across the threshold, and the
+    g_m / g_ds partials against central finite differences."""
+    md = np.zeros(1, dtype=mna.MOSFET_DTYPE)
+    md["drain"], md["gate"], md["source"] = 0, 1, mna.SENTINEL
+    md["polarity"], md["vto"], md["kp"], md["lam"] = 1.0, 0.7, 1.1e-4, 0.04
+    def ev(vd, vg):
+        i, gm, gds = devices_ref.mosfet_eval(md, np.array([vd, vg]))
+        return i[0], gm[0], gds[0]
+    i, _, _ = ev(1.0, 0.0)
+    assert abs(i) < 1e-12                                   # cutoff
+    kp = float(np.float32(1.1e-4)); lam = float(np.float32(0.04)); vto = float(np.float32(0.7))
+    i, _, _ = ev(3.0, 2.0)
+    vov = 2.0 - vto
+    assert abs(i - kp / 2 * vov * vov * (1 + lam * 3.0)) < 1e-9 * abs(i)   # saturation
+    a, _, _ = ev(1.0, vto - 1e-9); b, _, _ = ev(1.0, vto + 1e-9)
+    assert abs(a - b) < 1e-12                               # continuity
+    for (vd, vg) in ((0.2, 1.5), (2.0, 1.2), (1.0, 0.75), (0.05, 0.6)):
+        h = 1e-6
+        _, gm, gds = ev(vd, vg)
+        gm_fd = (ev(vd, vg + h)[0] - ev(vd, vg - h)[0]) / (2 * h)
+        gds_fd = (ev(vd + h, vg)[0] - ev(vd - h, vg)[0]) / (2 * h)
+        assert abs(gm - gm_fd) <= 1e-5 * max(abs(gm), 1e-9)
+        assert abs(gds - gds_fd) <= 1e-5 * max(abs(gds), 1e-9)
+    md["polarity"] = -1.0                                   # PMOS polarity
+    i_p, _, _ = devices_ref.mosfet_eval(md, np.array([-3.0, -2.0]))
+    assert i_p[0] < 0
+
+
+def test_pnjlim_reference_behaviour():
+    """Modified pnjlim (ds_nonlinear_shaders.rs:1173-1187)."""
+    vt = 0.02585
+    vcrit = vt * math.log(vt / (math.sqrt(2) * 1e-14))
+    assert devices_ref.pnjlim(0.3, 0.0, vt, vcrit) == 0.3            # below vcrit: unchanged
+    v = float(devices_ref.pnjlim(5.0, 0.6, vt, vcrit))
+    assert 0.6 < v < 5.0
+    assert abs(v - (0.6 + vt * (2 + math.log((1 + 4.4 / vt) - 2)))) < 1e-12
+    v2 = float(devices_ref.pnjlim(5.0, -1.0, vt, vcrit))
+    assert abs(v2 - vt * math.log(5.0 / vt)) < 1e-12
