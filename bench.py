@@ -1,0 +1,400 @@
+"""Benchmark: DC operating points per second of the 500x500 diode mesh
+(250,002 unknowns, 1.25 M nonzeros, 25,000 diodes) on one B200, mixed
+precision (FP32 Krylov bulk, FP64 device evaluation / residual / update)
+against the plain FP64 path, each checked against the FP64 oracle.
+
+One step = one complete DC Newton solve from x = 0: device evaluation,
+stamp-map assembly, BiCGSTAB, limiting and convergence, all inside one
+persistent kernel launch.  `value` uses a device-resident plan (inputs
+already in HBM); `e2e` calls the public C ABI entry point ohm_newton_solve
+with pinned host arrays every step (upload, solve, download).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: one process per GPU (torchrun); every rank solves its own replica
+(the path has no exchange step), value = all ranks' solves / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s & SpMV HBM GB/s: mixed-prec batched vs plain FP64 GPU at 1e-9 rel err"
+WORKLOAD = "diode-mesh 500x500 DC operating point (250,002 unknowns, 25,000 diodes, seed 1)"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--rows", type=int, default=500)
+    p.add_argument("--cols", type=int, default=500)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
+                   help="one warm-up and one timed solve only (for an ncu capture)")
+    return p.parse_args()
+
+
+def newton_params(mixed: bool):
+    from ohmnivore_b200 import solver as S
+    return S.NewtonParams(max_iterations=100, abs_tol=1e-10, bicgstab_max_iterations=20000,
+                          bicgstab_tolerance=1e-14, precision=1 if mixed else 0, inner_rtol=1e-4)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def spmv_bytes(n, nnz, wa, wv):
+    """Algorithmic SpMV bytes: values + column indices + row pointers + x read once + y write."""
+    return nnz * (wa + 4) + 4 * (n + 1) + 2 * n * wv
+
+
+def solve_bytes(info, n, nnz, nd, mixed):
+    """Algorithmic bytes of one persistent-kernel launch (one Newton solve).
+
+    Per Newton iteration: device evaluation + stamp map (descriptor 48 B,
+    anode voltage 8 B, 6 stamp values written and read 16 B each, the touched
+    slot's base + value 16 B, rhs base + value 16 B); the FP64 residual
+    b - J x (SpMV at FP64 + b read + r64 write + Krylov vectors initialised:
+    r, r_hat, p, v, d); the limiter (x, x_prev, scale, d: 4 n*8 + proposals).
+    Per BiCGSTAB iteration (Jacobi): 2 SpMV + 21 length-n vector streams +
+    2 diagonal reads, in the Krylov precision (4 B mixed, 8 B FP64).
+    """
+    w = 4 if mixed else 8
+    newton_it = int(info["iterations"])
+    kry = int(info["krylov_iterations"])
+    b_eval = nd * (48 + 8 + 6 * 16 + 16 + 16)
+    b_setup = spmv_bytes(n, nnz, 8, 8) + 2 * n * 8 + n * 8 + 5 * n * w + 2 * n * w
+    b_limit = 4 * n * 8 + nd * (48 + 16)
+    b_it = 2 * spmv_bytes(n, nnz, w, w) + 21 * n * w + 2 * n * w
+    return newton_it * (b_eval + b_setup + b_limit) + kry * b_it, kry
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args, rank):
+    """Reference arm: the oracle port of the reference CPU path (FP64 Newton
+    with a sparse LU per iteration, newton.rs CpuSparseLu mode) on the host."""
+    if rank != 0:
+        return
+    from ohmnivore_b200 import circuits, mna
+    from oracle import newton_ref
+    sysm = mna.compile_circuit(circuits.diode_mesh(args.rows, args.cols, seed=1))
+    t_w = time.perf_counter()
+    for _ in range(args.warmup):                       # warm-up: one Newton iteration each
+        try:
+            newton_ref.newton(sysm, max_iterations=1)
+        except Exception:
+            pass
+    t_w = time.perf_counter() - t_w
+    times = []
+    iters = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, it = newton_ref.newton(sysm)
+        times.append(time.perf_counter() - t0)
+        iters = it
+    total = sum(times)
+    value = args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "newton_iterations": iters},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+                             "sample": f"{args.steps} full DC solves of the workload (FP64 Newton + "
+                                       "SuperLU per iteration, single thread); warm-up = 1 Newton "
+                                       "iteration each"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if args.profile:
+        run_profile_case(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from ohmnivore_b200 import circuits, mna
+    from ohmnivore_b200 import solver as S
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+
+    sysm = mna.compile_circuit(circuits.diode_mesh(args.rows, args.cols, seed=1))
+    n, nnz, nd = sysm.size, sysm.g.nnz, len(sysm.diode_descriptors)
+    ctx = S.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.lib.ohm_ctx_stream(ctx.handle), device=local_rank)
+    plan = S.NewtonPlan(sysm, ctx)
+    x = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local_rank}")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def timed_solves(mixed, steps, warmup):
+        params = newton_params(mixed)
+        infos = []
+        for _ in range(warmup):
+            with torch.cuda.stream(stream):
+                x.zero_()
+            plan.newton_device(x.data_ptr(), params)
+        barrier()
+        total_ms = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()                       # L2 flush outside the timed interval
+                x.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            infos.append(plan.newton_device(x.data_ptr(), params))
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+        barrier()
+        t = torch.tensor([total_ms], dtype=torch.float64, device=x.device)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), infos, x.cpu().numpy()
+
+    # ---- mixed precision (headline) and plain FP64, device-resident ----
+    with ClockSampler(local_rank) as clk:
+        mixed_ms, mixed_infos, x_mixed = timed_solves(True, args.steps, args.warmup)
+    clocks = clk.summary()
+    fp64_ms, fp64_infos, x_fp64 = timed_solves(False, args.steps, args.warmup)
+
+    # ---- e2e: public C ABI, pinned host arrays, upload + solve + download ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_vals = pin(sysm.g.val.astype(np.float64))
+    h_col = pin(sysm.g.col.astype(np.uint32))
+    h_rp = pin(sysm.g.row_ptr.astype(np.uint32))
+    h_b = pin(sysm.b_dc.astype(np.float64))
+    h_dd = torch.from_numpy(sysm.diode_descriptors.view(np.uint8)).pin_memory().numpy().view(mna.DIODE_DTYPE)
+    h_x = pin(np.zeros(n))
+    params = newton_params(True)
+
+    def e2e_call():
+        return S.newton_solve(ctx, h_vals, h_col, h_rp, h_b, h_dd, sysm.bjt_descriptors,
+                              sysm.mosfet_descriptors, n, nnz, params)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_call()
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        h_x[:] = e2e_call()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    barrier()
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=x.device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    h2d = h_vals.nbytes + h_col.nbytes + h_rp.nbytes + h_b.nbytes + h_dd.nbytes
+    d2h = n * 8
+
+    # ---- SpMV bandwidth (cold L2, FP64 and FP32 values) ----
+    spmv = spmv_roofline(S, ctx, sysm, stream, flush)
+
+    # ---- roofline of the persistent kernel (dominant: the only kernel of a solve) ----
+    peaks = measured_peaks()
+    hbm_peak = peaks["hbm_gbs"] if peaks else 6650.0
+    peak_src = "measured" if peaks else "fallback"
+    info0 = mixed_infos[-1]
+    algo_bytes, kry = solve_bytes(info0, n, nnz, nd, mixed=True)
+    per_launch_ms = mixed_ms / args.steps
+    achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+
+    value = world * args.steps / (mixed_ms * 1e-3)
+    fp64_value = world * args.steps / (fp64_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 Krylov / f64 Newton", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "mixed (FP32 BiCGSTAB bulk, FP64 eval/residual/update)",
+                   "preconditioner": "block Jacobi (2x2 for the source branch row)",
+                   "newton_abs_tol": 1e-10, "krylov_tol_floor": 1e-14, "inner_rtol": 1e-4,
+                   "l2": "flushed (512 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "plain_fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": fp64_ms / args.steps,
+                       "newton_iterations": fp64_infos[-1]["iterations"],
+                       "krylov_iterations": fp64_infos[-1]["krylov_iterations"]},
+        "mixed_vs_fp64": value / fp64_value,
+        "newton_iterations": info0["iterations"], "krylov_iterations": kry,
+        "fp64_fallbacks": info0["fp64_fallbacks"], "krylov_restarts": info0["krylov_restarts"],
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "api": "ohm_newton_solve (host arrays in pinned memory)"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                     "kernel": "persistent_solver<float,2>",
+                     "algorithmic_bytes_per_launch": algo_bytes,
+                     "note": "working set (~40 MB) is L2-resident inside a solve"},
+        "spmv": spmv,
+        "clocks": clocks,
+    }
+
+    # ---- accuracy vs the FP64 oracle and the CPU baseline (rank 0, N = 1) ----
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import newton_ref
+        t0 = time.perf_counter()
+        ref, it_ref = newton_ref.newton(sysm)
+        cpu_s = time.perf_counter() - t0
+        nn = slice(0, sysm.n_nodes)
+        br = slice(sysm.n_nodes, n)
+        err = lambda a, sl: float(np.max(np.abs(a[sl] - ref[sl])) / np.max(np.abs(ref[sl])))  # noqa: E731
+        line["rel_err_vs_oracle"] = {
+            "mixed": {"voltages": err(x_mixed, nn), "currents": err(x_mixed, br)},
+            "fp64": {"voltages": err(x_fp64, nn), "currents": err(x_fp64, br)},
+            "e2e_mixed": {"voltages": err(h_x, nn), "currents": err(h_x, br)}}
+        line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": f"1 full DC solve of the workload ({it_ref} FP64 Newton "
+                                          "iterations, SuperLU per iteration), single thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_profile_case(args):
+    """Profiling case: one warm-up solve and one solve of the workload."""
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    from ohmnivore_b200 import solver as S
+    sysm = mna.compile_circuit(circuits.diode_mesh(args.rows, args.cols, seed=1))
+    ctx = S.Context(0)
+    plan = S.NewtonPlan(sysm, ctx)
+    x = torch.zeros(sysm.size, dtype=torch.float64, device="cuda")
+    params = newton_params(args.profile == "mixed")
+    for _ in range(2):
+        x.zero_()
+        torch.cuda.synchronize()
+        info = plan.newton_device(x.data_ptr(), params)
+    print(json.dumps({"profile_case": f"diode-mesh {args.rows}x{args.cols}", "precision": args.profile,
+                      **info}))
+    plan.close()
+    ctx.close()
+
+
+def spmv_roofline(S, ctx, sysm, stream, flush):
+    """Stand-alone CSR SpMV (the backend op) on the workload matrix, L2
+    flushed before every launch; algorithmic bytes / event time."""
+    import torch
+    be = S.SolverBackend(ctx)
+    A = be.upload_matrix(sysm.g)
+    bx = be.new_buffer(sysm.size)
+    by = be.new_buffer(sysm.size)
+    bx.upload(np.ones(sysm.size))
+    reps = 20
+    ms = []
+    for r in range(reps + 3):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        be.spmv(A, bx, by)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        if r >= 3:
+            ms.append(e0.elapsed_time(e1))
+    t = statistics.median(ms) * 1e-3
+    byt = spmv_bytes(sysm.size, sysm.g.nnz, 8, 8)
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    return {"kernel": "spmv_warp_kernel (FP64)", "bytes": byt, "us": t * 1e6, "achieved_gbs": byt / t / 1e9,
+            "frac": byt / t / 1e9 / peak, "cold_l2": True}
+
+
+if __name__ == "__main__":
+    main()

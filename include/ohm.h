@@ -95,7 +95,8 @@ typedef struct {                 /* BiCgStabParams (src/solver/bicgstab.rs:14-27
     int32_t precision;           /* ohm_precision */
     int32_t precond;             /* ohm_precond */
     double inner_rtol;           /* mixed: inner FP32 solve also stops at inner_rtol*||r0||; 0 = off */
-    int32_t max_refinements;     /* mixed: FP64 iterative-refinement sweeps (>= 1) */
+    int32_t max_refinements;     /* linear solves: FP64 iterative-refinement sweeps (>= 1);
+                                    > 1 also requires the FP64 residual to meet the tolerance */
     int32_t max_restarts;        /* restarts with r_hat = r after a rho or r_hat.v breakdown;
                                     0 = the reference's breakdown error; default 50 */
 } ohm_krylov_params;
@@ -114,6 +115,8 @@ typedef struct {
     int32_t iterations;          /* Newton iterations (or Krylov iterations for linear solves) */
     int32_t error_iteration;     /* NewtonNumericalError{iteration} */
     int64_t krylov_iterations;   /* total BiCGSTAB iterations */
+    int32_t fp64_fallbacks;      /* mixed: FP32 Krylov solves redone in FP64 */
+    int32_t krylov_restarts;     /* BiCGSTAB restarts after a breakdown */
     double max_residual;         /* last max|x - x_old| (NewtonNotConverged{max_residual}) */
     double final_residual_norm;  /* ||b - A x||_2 at exit (FP64), when computed */
     double b_norm;               /* ||b||_2 of the last linear system */
@@ -133,7 +136,9 @@ typedef struct ohm_plan ohm_plan;    /* device-resident nonlinear system (Newton
 const char *ohm_last_error(void);
 const char *ohm_version(void);
 
-/* One context = one CUDA device + one stream (WgpuDsBackend::new, ds_backend.rs). */
+/* One context = one CUDA device + one stream (WgpuDsBackend::new, ds_backend.rs).
+ * Destroying a context while plans, buffers or matrices created on it are
+ * alive is allowed: the context is released when the last of them is. */
 ohm_status ohm_ctx_create(int device, ohm_ctx **out);
 ohm_status ohm_ctx_destroy(ohm_ctx *ctx);
 ohm_status ohm_ctx_synchronize(ohm_ctx *ctx);

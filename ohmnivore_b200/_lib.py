@@ -34,6 +34,7 @@ class NewtonParamsC(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("krylov_code", C.c_int32), ("iterations", C.c_int32),
                 ("error_iteration", C.c_int32), ("krylov_iterations", C.c_int64),
+                ("fp64_fallbacks", C.c_int32), ("krylov_restarts", C.c_int32),
                 ("max_residual", C.c_double), ("final_residual_norm", C.c_double),
                 ("b_norm", C.c_double), ("kernel_launches", C.c_int64)]
 

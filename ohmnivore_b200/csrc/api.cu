@@ -59,6 +59,8 @@ extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
 }
 
 // ---------------------------------------------------------------- context --
+static void ctx_free(ohm_ctx *c);
+
 extern "C" ohm_status ohm_ctx_create(int device, ohm_ctx **out) {
     if (!out) return fail(OHM_ERR_INVALID_ARG, "out is null");
     *out = nullptr;
@@ -79,15 +81,14 @@ extern "C" ohm_status ohm_ctx_create(int device, ohm_ctx **out) {
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->info_host, sizeof(DeviceInfo));
     if (e == cudaSuccess) e = dalloc(&c->dot_scratch, 2048);
     if (e != cudaSuccess) {
-        ohm_ctx_destroy(c);
+        ctx_free(c);
         return fail(OHM_ERR_CUDA, "context setup failed: %s", cudaGetErrorString(e));
     }
     *out = c;
     return OHM_OK;
 }
 
-extern "C" ohm_status ohm_ctx_destroy(ohm_ctx *c) {
-    if (!c) return OHM_OK;
+static void ctx_free(ohm_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->sync_words);
@@ -96,7 +97,22 @@ extern "C" ohm_status ohm_ctx_destroy(ohm_ctx *c) {
     cudaFree(c->dot_scratch);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+}
+
+extern "C" ohm_status ohm_ctx_destroy(ohm_ctx *c) {
+    if (!c) return OHM_OK;
+    if (c->live_objects > 0) {
+        c->destroy_pending = true;    // released when the last object goes
+        return OHM_OK;
+    }
+    ctx_free(c);
     return OHM_OK;
+}
+
+void ohm_ctx_retain(ohm_ctx *c) { ++c->live_objects; }
+
+void ohm_ctx_release(ohm_ctx *c) {
+    if (--c->live_objects == 0 && c->destroy_pending) ctx_free(c);
 }
 
 extern "C" ohm_status ohm_ctx_synchronize(ohm_ctx *c) {
@@ -210,15 +226,14 @@ static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, co
 // ------------------------------------------------------------ launch logic --
 using KernelFn = void (*)(KernelArgs);
 
-template <typename T>
 static KernelFn pick_kernel(int lpr) {
     switch (lpr) {
-        case 1: return persistent_solver<T, 1>;
-        case 2: return persistent_solver<T, 2>;
-        case 4: return persistent_solver<T, 4>;
-        case 8: return persistent_solver<T, 8>;
-        case 16: return persistent_solver<T, 16>;
-        default: return persistent_solver<T, 32>;
+        case 1: return persistent_solver<1>;
+        case 2: return persistent_solver<2>;
+        case 4: return persistent_solver<4>;
+        case 8: return persistent_solver<8>;
+        case 16: return persistent_solver<16>;
+        default: return persistent_solver<32>;
     }
 }
 
@@ -234,9 +249,9 @@ static int choose_lpr(int64_t n, int64_t nnz) {
 
 static constexpr int kBlock = 512;
 
-static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, bool mixed, int64_t nnz, int *launches) {
+static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, int64_t nnz, int *launches) {
     const int lpr = choose_lpr(a.n, nnz);
-    KernelFn fn = mixed ? pick_kernel<float>(lpr) : pick_kernel<double>(lpr);
+    KernelFn fn = pick_kernel(lpr);
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
     if (per_sm < 1) return fail(OHM_ERR_CUDA, "solver kernel does not fit on an SM");
@@ -296,6 +311,8 @@ static ohm_status finish_solver(ohm_ctx *c, ohm_solve_info *info, int launches) 
         info->iterations = di.iterations;
         info->error_iteration = di.error_iteration;
         info->krylov_iterations = di.krylov_iterations;
+        info->fp64_fallbacks = di.fp64_fallbacks;
+        info->krylov_restarts = di.krylov_restarts;
         info->max_residual = di.max_residual;
         info->final_residual_norm = di.final_residual;
         info->b_norm = di.b_norm;
@@ -311,18 +328,20 @@ struct Workspace {
     int64_t n = 0;
     double *vec = nullptr;       // 12 * n doubles
     double *r64 = nullptr;
+    double *dx = nullptr;
     double *partials = nullptr;  // 8 * max grid
     int32_t *partner = nullptr;
     uint32_t *diag_slot = nullptr, *off_slot = nullptr;
     void release() {
-        cudaFree(vec); cudaFree(r64); cudaFree(partials);
+        cudaFree(vec); cudaFree(r64); cudaFree(dx); cudaFree(partials);
         cudaFree(partner); cudaFree(diag_slot); cudaFree(off_slot);
-        vec = r64 = partials = nullptr; partner = nullptr; diag_slot = off_slot = nullptr;
+        vec = r64 = dx = partials = nullptr; partner = nullptr; diag_slot = off_slot = nullptr;
     }
     cudaError_t alloc(int64_t n_, int num_sms) {
         n = n_;
         cudaError_t e = dalloc(&vec, 12 * (size_t)n);
         if (e == cudaSuccess) e = dalloc(&r64, n);
+        if (e == cudaSuccess) e = dalloc(&dx, n);
         if (e == cudaSuccess) e = dalloc(&partials, 8 * (size_t)num_sms * 8);
         if (e == cudaSuccess) e = dalloc(&partner, n);
         if (e == cudaSuccess) e = dalloc(&diag_slot, n);
@@ -334,6 +353,7 @@ struct Workspace {
                           &a.pc_self, &a.pc_part};
         for (int k = 0; k < 12; ++k) *slots[k] = (void *)(vec + (size_t)k * n);
         a.r64 = r64;
+        a.dx = dx;
         a.partials = partials;
         a.partner = partner;
         a.diag_slot = diag_slot;
@@ -394,14 +414,14 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     a.precond = p->precond == OHM_PRECOND_NONE ? kPcNone : (p->precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
     ws.bind(a);
     a.newton = 0;
-    a.max_outer = mixed ? std::max(1, p->max_refinements) : 1;
+    a.mixed = mixed ? 1 : 0;
+    a.max_outer = std::max(1, p->max_refinements);
     a.max_krylov = p->max_iterations;
     a.krylov_tol = p->tolerance;
     a.inner_rtol = mixed ? (p->inner_rtol > 0.0 ? p->inner_rtol : 1e-4) : p->inner_rtol;
-    a.accept_partial = mixed ? 1 : 0;
-    a.require_true_residual = mixed ? 1 : 0;
+    a.require_true_residual = p->max_refinements > 1 ? 1 : 0;
     a.max_restarts = std::max(0, p->max_restarts);
-    st = launch_solver(c, a, mixed, nnz, &launches);
+    st = launch_solver(c, a, nnz, &launches);
     if (st == OHM_OK) st = finish_solver(c, info, launches);
     cudaStreamSynchronize(c->stream);
     ws.release();
@@ -587,15 +607,18 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
         plan_free(p);
         return fail(OHM_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e));
     }
+    ohm_ctx_retain(c);
     *out = p;
     return OHM_OK;
 }
 
 extern "C" ohm_status ohm_plan_destroy(ohm_plan *p) {
     if (!p) return OHM_OK;
-    cudaSetDevice(p->ctx->device);
-    cudaStreamSynchronize(p->ctx->stream);
+    ohm_ctx *c = p->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
     plan_free(p);
+    ohm_ctx_release(c);
     return OHM_OK;
 }
 
@@ -648,8 +671,8 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.max_krylov = kp.max_iterations;
     a.krylov_tol = kp.tolerance;
     const bool mixed = kp.precision == OHM_PREC_MIXED;
+    a.mixed = mixed ? 1 : 0;
     a.inner_rtol = mixed ? (kp.inner_rtol > 0.0 ? kp.inner_rtol : 1e-4) : kp.inner_rtol;
-    a.accept_partial = mixed ? 1 : 0;
     a.max_restarts = std::max(0, kp.max_restarts);
     return OHM_OK;
 }
@@ -675,7 +698,7 @@ extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const o
     st = plan_args(p, np, x_dev, a);
     if (st != OHM_OK) return st;
     int launches = 0;
-    st = launch_solver(c, a, np->krylov.precision == OHM_PREC_MIXED, p->nnz, &launches);
+    st = launch_solver(c, a, p->nnz, &launches);
     if (st != OHM_OK) return st;
     return finish_solver(c, info, launches);
 }

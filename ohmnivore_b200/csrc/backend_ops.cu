@@ -75,16 +75,19 @@ extern "C" ohm_status ohm_buf_create(ohm_ctx *c, int64_t n, ohm_buf **out) {
         delete b;
         return ohm_fail(OHM_ERR_CUDA, "buffer allocation: %s", cudaGetErrorString(e));
     }
+    ohm_ctx_retain(c);
     *out = b;
     return OHM_OK;
 }
 
 extern "C" ohm_status ohm_buf_destroy(ohm_buf *b) {
     if (!b) return OHM_OK;
-    cudaSetDevice(b->ctx->device);
-    cudaStreamSynchronize(b->ctx->stream);
+    ohm_ctx *c = b->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
     cudaFree(b->d);
     delete b;
+    ohm_ctx_release(c);
     return OHM_OK;
 }
 
@@ -130,6 +133,7 @@ extern "C" ohm_status ohm_csr_upload(ohm_ctx *c, int64_t n, int64_t nnz, const u
         delete m;
         return ohm_fail(OHM_ERR_CUDA, "CSR upload: %s", cudaGetErrorString(e));
     }
+    ohm_ctx_retain(c);
     *out = m;
     return OHM_OK;
 }
@@ -144,10 +148,12 @@ extern "C" ohm_status ohm_csr_update_values(ohm_ctx *c, ohm_csr *m, const double
 
 extern "C" ohm_status ohm_csr_destroy(ohm_csr *m) {
     if (!m) return OHM_OK;
-    cudaSetDevice(m->ctx->device);
-    cudaStreamSynchronize(m->ctx->stream);
+    ohm_ctx *c = m->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
     cudaFree(m->rp); cudaFree(m->col); cudaFree(m->val);
     delete m;
+    ohm_ctx_release(c);
     return OHM_OK;
 }
 

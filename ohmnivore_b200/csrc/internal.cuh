@@ -32,7 +32,15 @@ struct ohm_ctx {
     DeviceInfo *info_dev = nullptr;
     DeviceInfo *info_host = nullptr;      // pinned
     double *dot_scratch = nullptr;        // for ohm_dot
+    // Objects created on this context (plans, buffers, matrices).  Destroying
+    // the context while some are alive defers the release to the last one.
+    int live_objects = 0;
+    bool destroy_pending = false;
 };
+
+// Child-object bookkeeping (see ohm_ctx::live_objects).
+void ohm_ctx_retain(ohm_ctx *c);
+void ohm_ctx_release(ohm_ctx *c);
 
 struct ohm_buf {
     ohm_ctx *ctx;

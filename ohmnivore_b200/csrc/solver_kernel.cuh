@@ -1,14 +1,22 @@
 // Persistent solver kernel: the whole Newton loop (device evaluation, MNA
 // stamping through the stamp map, FP64 residual, right-preconditioned
-// BiCGSTAB, voltage limiting, convergence test) or a single linear solve
-// with FP64 iterative refinement, in ONE cooperative launch.
+// BiCGSTAB, voltage limiting, convergence test) or a linear solve with FP64
+// iterative refinement, in ONE cooperative launch.
 //
 // Algorithms followed:
 //   Newton loop       src/solver/newton.rs:153-488 (newton_solve)
 //   BiCGSTAB          src/solver/bicgstab.rs:56-189 (bicgstab_with_params),
-//                     same operation order and breakdown tests (1e-30)
+//                     same operation order; breakdown tests made scale-free
+//                     (see krylov()) and optionally followed by a restart
 //   Jacobi            src/solver/gpu.rs:177-190, newton.rs:340-361
 //   convergence       src/solver/ds_nonlinear_shaders.rs:1256-1297
+//
+// Each outer iteration solves the correction equation J d = b - J x in the
+// Krylov precision (FP32 or FP64) and updates x in FP64.  With the reference's
+// stopping rule ||b - J x_new|| < tol ||b|| (bicgstab.rs:98, 161) this is the
+// reference's linear solve with a warm start; mixed precision adds an inner
+// relative tolerance and falls back to an FP64 Krylov solve when the FP32 one
+// fails or stalls (contraction worse than 0.5).
 //
 // Work split: block b owns rows [b*n/G, (b+1)*n/G).  Vector phases map one
 // thread per row; SpMV phases map LPR lanes per row (sub-warp CSR).  Device
@@ -19,6 +27,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 #include "devices.cuh"
@@ -26,6 +35,7 @@
 namespace ohm {
 
 enum KrylovCode : int {
+    kKrylovAbort = -1,        // a barrier gave up; leave the kernel
     kKrylovRunning = 0,
     kKrylovConverged = 1,
     kKrylovMaxIter = 2,
@@ -46,12 +56,19 @@ enum SolveStatus : int {
 
 enum PrecondKind : int { kPcAuto = 0, kPcJacobi = 1, kPcIsai = 2, kPcNone = 3 };
 
+// Breakdown test: |(a, b)| < kBreakdownRel * ||a|| ||b||.  The reference's
+// absolute 1e-30 (bicgstab.rs:107, :125) depends on the units of the
+// residual; a relative test only fires on (near-)exact orthogonality.
+constexpr double kBreakdownRel = 1e-24;
+
 struct DeviceInfo {
     int status;
     int krylov_code;
-    int iterations;          // Newton iterations, or IR sweeps for a linear solve
+    int iterations;          // Newton iterations, or refinement sweeps for a linear solve
     int error_iteration;
     long long krylov_iterations;
+    int fp64_fallbacks;      // mixed precision: Krylov solves redone in FP64
+    int krylov_restarts;
     double max_residual;     // last max|x - x_old|
     double final_residual;   // ||b - A x||_2 (FP64) at exit, linear mode
     double b_norm;
@@ -69,15 +86,16 @@ struct KernelArgs {
     double *x;                  // FP64 iterate (in: initial guess, out: solution)
     double *x_prev;             // FP64 previous Newton iterate
     double *r64;                // FP64 residual b - A x
+    double *dx;                 // FP64 correction from the Krylov solve
 
     // block-Jacobi preconditioner (1x1, or 2x2 pairs for zero-diagonal rows)
     int precond;
     const int32_t *partner;     // -1: unpaired
     const uint32_t *diag_slot;  // CSR slot of (i,i), kSentinel if absent
     const uint32_t *off_slot;   // CSR slot of (i, partner(i))
-    void *pc_self, *pc_part;    // T arrays
+    void *pc_self, *pc_part;    // Krylov-precision arrays
 
-    // Krylov vectors (T arrays); p is double-buffered (p0/p1)
+    // Krylov vectors (8-byte slots; used as float or double); p is double-buffered
     void *r, *rhat, *p0, *p1, *v, *s, *t, *phat, *shat, *d;
 
     // nonlinear devices and the stamp map
@@ -94,19 +112,37 @@ struct KernelArgs {
     unsigned long long *node_scale;
 
     // control
-    int newton;                 // 1: Newton loop, 0: linear solve (+ IR)
-    int max_outer;              // Newton iterations or IR sweeps
+    int newton;                 // 1: Newton loop, 0: linear solve (+ refinement)
+    int mixed;                  // 1: FP32 Krylov with FP64 fallback
+    int max_outer;              // Newton iterations or refinement sweeps
     double abs_tol, rel_tol;    // Newton convergence
     int max_krylov;
     double krylov_tol;          // ||r|| < krylov_tol * ||b||  (bicgstab.rs:98)
-    double inner_rtol;          // ... or < inner_rtol * ||r0|| (mixed inner solve)
-    int accept_partial;         // mixed: accept a max-iteration inner solve that reduced ||r||
-    int max_restarts;           // restarts with r_hat = r after a rho / (r_hat,v) breakdown
+    double inner_rtol;          // ... or < inner_rtol * ||r0|| (inexact inner solve)
+    int max_restarts;           // restarts with r_hat = r after a breakdown
+    int require_true_residual;  // linear: fail unless the FP64 residual meets the tolerance
 
     double *partials;           // >= 8 * gridDim.x doubles (two alternating regions)
-    int require_true_residual;  // linear: fail unless the FP64 residual meets the tolerance
     GridSync gs;
     DeviceInfo *info;
+};
+
+// Per-block view of the launch: row range and the reduction buffers.
+struct Grid {
+    int G, bid, r0, r1, gtid, gstride;
+    double *smem;
+    double *partials;
+    int red;
+    GridSync gs;
+
+    // Consecutive grid reductions alternate between two partial regions: a
+    // block may publish reduction j+1 while a slower block still reads
+    // reduction j, but never reduction j+2 (a barrier separates them).
+    __device__ __forceinline__ double *part() {
+        double *p = partials + (size_t)(red & 1) * 4 * G;
+        ++red;
+        return p;
+    }
 };
 
 template <typename T>
@@ -138,36 +174,239 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
     }
 }
 
-template <typename T, int LPR>
-__global__ void __launch_bounds__(512) persistent_solver(KernelArgs a) {
-    __shared__ double smem[32 * 4];
-    const int G = gridDim.x, bid = blockIdx.x;
-    const int n = a.n;
-    const int r0 = (int)(((long long)n * bid) / G);
-    const int r1 = (int)(((long long)n * (bid + 1)) / G);
-    const int gtid = bid * blockDim.x + threadIdx.x;
-    const int gstride = G * blockDim.x;
+#define OHM_SYNC_OR(ret)                          \
+    do {                                          \
+        if (!grid_barrier(g.gs)) return ret;      \
+    } while (0)
 
+struct KrylovOut {
+    int iterations;
+    int restarts;
+};
+
+// Right-preconditioned BiCGSTAB on J d = r64 in precision T, d0 = 0.
+// Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On success the
+// correction is left in a.dx (FP64) for the rows of this block.
+template <typename T, int LPR>
+__device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
+                                   bool accept_partial, KrylovOut &out) {
+    const int r0 = g.r0, r1 = g.r1;
     T *r = (T *)a.r, *rhat = (T *)a.rhat, *v = (T *)a.v, *s = (T *)a.s, *t = (T *)a.t;
     T *phat = (T *)a.phat, *shat = (T *)a.shat, *d = (T *)a.d;
     T *pc_self = (T *)a.pc_self, *pc_part = (T *)a.pc_part;
     T *pin = (T *)a.p0, *pout = (T *)a.p1;
-    const T *A = nullptr;
+    const T *A;
     if constexpr (sizeof(T) == 4) A = (const T *)a.vals32; else A = (const T *)a.vals64;
+    out.iterations = 0;
+    out.restarts = 0;
 
-    // Consecutive grid reductions alternate between two partial regions: a
-    // block may publish reduction j+1 while a slower block still reads
-    // reduction j, but never reduction j+2 (a barrier separates them).
-    int red = 0;
-    auto part = [&]() { double *p = a.partials + (size_t)(red & 1) * 4 * G; ++red; return p; };
+    // ---- start: r = r64, r_hat = r, p = v = d = 0; preconditioner coefficients ----
+    double acc0[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const T rt = cvt<T>(a.r64[i]);
+        r[i] = rt; rhat[i] = rt; pin[i] = T(0); v[i] = T(0); d[i] = T(0);
+        acc0[0] += (double)rt * (double)rt;
+        double cs = 0.0, cp = 0.0;
+        if (a.precond != kPcNone) {
+            const uint32_t ds = a.diag_slot[i];
+            const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
+            const int pi = a.partner[i];
+            if (a.precond == kPcAuto && pi >= 0) {
+                const double akk = a.diag_slot[pi] == kSentinel ? 0.0 : a.vals64[a.diag_slot[pi]];
+                const double aik = a.vals64[a.off_slot[i]];
+                const double aki = a.vals64[a.off_slot[pi]];
+                const double det = aii * akk - aik * aki;
+                if (fabs(det) > 1e-300) { cs = akk / det; cp = -aik / det; }
+            } else if (fabs(aii) > 1e-30) {
+                cs = 1.0 / aii;
+            } else if (a.precond == kPcAuto) {
+                cs = 1.0;   // unpaired zero diagonal: identity keeps M^-1 nonsingular
+            }
+        } else {
+            cs = 1.0;
+        }
+        pc_self[i] = cvt<T>(cs);
+        pc_part[i] = cvt<T>(cp);
+    }
+    {
+        double *pr = g.part();
+        publish_partials<1>(acc0, pr, g.smem);
+        OHM_SYNC_OR(kKrylovAbort);
+        gather_partials<1>(pr, acc0, g.smem);
+    }
+    const double r0norm = sqrt(acc0[0]);
+    const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
+    double rr_cur = acc0[0];          // ||r||^2
+    double rhat2 = acc0[0];           // ||r_hat||^2
+    double rho_new = acc0[0];         // (r_hat, r)
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    int code = kKrylovRunning;
+    int it = 0;
+    if (!isfinite(r0norm)) {
+        code = kKrylovNan;
+    } else if (r0norm < abs_tol || r0norm == 0.0) {
+        code = kKrylovConverged;
+    } else {
+        for (; it < a.max_krylov; ++it) {
+            if (!(fabs(rho_new) >= kBreakdownRel * sqrt(rhat2 * rr_cur))) {
+                if (out.restarts < a.max_restarts && rr_cur > 0.0) {
+                    // restart: the shadow residual r_hat = b (bicgstab.rs:87) can be
+                    // orthogonal to later residuals when b lives on a few source rows
+                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                        rhat[i] = r[i]; pin[i] = T(0); v[i] = T(0);
+                    }
+                    OHM_SYNC_OR(kKrylovAbort);
+                    rho = 1.0; alpha = 1.0; omega = 1.0;
+                    rho_new = rr_cur; rhat2 = rr_cur;
+                    ++out.restarts;
+                } else {
+                    code = kKrylovBreakRho;
+                    break;
+                }
+            }
+            const double beta = (rho_new / rho) * (alpha / omega);
+            rho = rho_new;
+            // p = (p - omega v) * beta + r ; phat = M^-1 p
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const T pt = cvt<T>(((double)pin[i] + (-omega) * (double)v[i]) * beta + (double)r[i]);
+                pout[i] = pt;
+                double z = (double)pc_self[i] * (double)pt;
+                const int pi = a.partner[i];
+                if (pi >= 0) {
+                    const T pk = cvt<T>(((double)pin[pi] + (-omega) * (double)v[pi]) * beta + (double)r[pi]);
+                    z += (double)pc_part[i] * (double)pk;
+                }
+                phat[i] = cvt<T>(z);
+            }
+            { T *tmp = pin; pin = pout; pout = tmp; }
+            OHM_SYNC_OR(kKrylovAbort);
+            // v = A phat ; (r_hat, v), (v, v)
+            double acc1[2] = {0.0, 0.0};
+            spmv_rows<LPR>(a.row_ptr, a.col, A, phat, r0, r1, [&](int i, double y) {
+                const T yt = cvt<T>(y);
+                v[i] = yt;
+                acc1[0] += (double)rhat[i] * (double)yt;
+                acc1[1] += (double)yt * (double)yt;
+            });
+            {
+                double *pr = g.part();
+                publish_partials<2>(acc1, pr, g.smem);
+                OHM_SYNC_OR(kKrylovAbort);
+                gather_partials<2>(pr, acc1, g.smem);
+            }
+            if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
+                if (out.restarts < a.max_restarts && rr_cur > 0.0) {
+                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                        rhat[i] = r[i]; pin[i] = T(0); v[i] = T(0);
+                    }
+                    OHM_SYNC_OR(kKrylovAbort);
+                    rho = 1.0; alpha = 1.0; omega = 1.0;
+                    rho_new = rr_cur; rhat2 = rr_cur;
+                    ++out.restarts;
+                    continue;
+                }
+                code = kKrylovBreakRv;
+                break;
+            }
+            alpha = rho / acc1[0];
+            // s = r - alpha v ; shat = M^-1 s ; ||s||^2
+            double acc2[1] = {0.0};
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const T st = cvt<T>((double)r[i] + (-alpha) * (double)v[i]);
+                s[i] = st;
+                acc2[0] += (double)st * (double)st;
+                double z = (double)pc_self[i] * (double)st;
+                const int pi = a.partner[i];
+                if (pi >= 0) {
+                    const T sk = cvt<T>((double)r[pi] + (-alpha) * (double)v[pi]);
+                    z += (double)pc_part[i] * (double)sk;
+                }
+                shat[i] = cvt<T>(z);
+            }
+            {
+                double *pr = g.part();
+                publish_partials<1>(acc2, pr, g.smem);
+                OHM_SYNC_OR(kKrylovAbort);
+                gather_partials<1>(pr, acc2, g.smem);
+            }
+            if (sqrt(acc2[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+                    d[i] = cvt<T>((double)d[i] + alpha * (double)phat[i]);
+                code = kKrylovConverged;
+                ++it;
+                break;
+            }
+            // t = A shat ; (t, s), (t, t)
+            double acc3[2] = {0.0, 0.0};
+            spmv_rows<LPR>(a.row_ptr, a.col, A, shat, r0, r1, [&](int i, double y) {
+                const T yt = cvt<T>(y);
+                t[i] = yt;
+                acc3[0] += (double)yt * (double)s[i];
+                acc3[1] += (double)yt * (double)yt;
+            });
+            {
+                double *pr = g.part();
+                publish_partials<2>(acc3, pr, g.smem);
+                OHM_SYNC_OR(kKrylovAbort);
+                gather_partials<2>(pr, acc3, g.smem);
+            }
+            if (!(acc3[1] > 0.0)) { code = kKrylovBreakTt; break; }
+            omega = acc3[0] / acc3[1];
+            // d += alpha phat ; d += omega shat ; r = s - omega t
+            double acc4[2] = {0.0, 0.0};
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                d[i] = cvt<T>(((double)d[i] + alpha * (double)phat[i]) + omega * (double)shat[i]);
+                const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
+                r[i] = rt;
+                acc4[0] += (double)rhat[i] * (double)rt;
+                acc4[1] += (double)rt * (double)rt;
+            }
+            {
+                double *pr = g.part();
+                publish_partials<2>(acc4, pr, g.smem);
+                OHM_SYNC_OR(kKrylovAbort);
+                gather_partials<2>(pr, acc4, g.smem);
+            }
+            rho_new = acc4[0];
+            rr_cur = acc4[1];
+            const double rnorm = sqrt(acc4[1]);
+            if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
+            if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
+            if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }
+            if (accept_partial && it + 1 == a.max_krylov && rnorm <= 0.5 * r0norm) {
+                code = kKrylovConverged;          // inexact inner solve accepted
+                ++it;
+                break;
+            }
+        }
+        if (code == kKrylovRunning) code = kKrylovMaxIter;
+    }
+    out.iterations = it;
+    if (code == kKrylovConverged)
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.dx[i] = (double)d[i];
+    return code;
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
+    __shared__ double smem[32 * 4];
+    Grid g;
+    g.G = gridDim.x;
+    g.bid = blockIdx.x;
+    g.r0 = (int)(((long long)a.n * g.bid) / g.G);
+    g.r1 = (int)(((long long)a.n * (g.bid + 1)) / g.G);
+    g.gtid = g.bid * blockDim.x + threadIdx.x;
+    g.gstride = g.G * blockDim.x;
+    g.smem = smem;
+    g.partials = a.partials;
+    g.red = 0;
+    g.gs = a.gs;
+    const int r0 = g.r0, r1 = g.r1, gtid = g.gtid, gstride = g.gstride;
+
     int status = kOk, kcode = kKrylovRunning, outer_done = 0, err_iter = 0;
+    int fallbacks = 0, restarts = 0;
     long long kiters = 0;
     double last_dmax = 0.0, bnorm_last = 0.0, final_res = -1.0;
-
-#define OHM_SYNC()                         \
-    do {                                   \
-        if (!grid_barrier(a.gs)) return;   \
-    } while (0)
 
     for (int outer = 0; outer < a.max_outer; ++outer) {
         // ---------------- device evaluation + stamping (Newton) ----------------
@@ -188,7 +427,7 @@ __global__ void __launch_bounds__(512) persistent_solver(KernelArgs a) {
                                   a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)a.nq + 2 * (size_t)m);
                 }
             }
-            OHM_SYNC();
+            OHM_SYNC_OR();
             // stamp map: each touched slot / row = base + contributions in canonical order
             for (int k = gtid; k < a.n_mslots + a.n_rrows; k += gstride) {
                 if (k < a.n_mslots) {
@@ -205,234 +444,85 @@ __global__ void __launch_bounds__(512) persistent_solver(KernelArgs a) {
                     a.b[row] = acc;
                 }
             }
-            OHM_SYNC();
+            OHM_SYNC_OR();
         }
 
-        // ------------- preconditioner, FP64 residual, Krylov start -------------
+        // -------------------------- FP64 residual r64 = b - A x -------------------------
+        double acc[3] = {0.0, 0.0, 0.0};   // ||b||^2, ||r||^2, #non-finite
+        spmv_rows<LPR>(a.row_ptr, a.col, a.vals64, a.x, r0, r1, [&](int i, double ax) {
+            const double bi = a.b[i];
+            const double ri = bi - ax;
+            a.r64[i] = ri;
+            acc[0] += bi * bi;
+            acc[1] += ri * ri;
+            if (!isfinite(ri)) acc[2] += 1.0;
+        });
         {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};   // ||b||^2, ||r||^2, (rhat, r), #non-finite
-            spmv_rows<LPR>(a.row_ptr, a.col, a.vals64, a.x, r0, r1, [&](int i, double ax) {
-                const double bi = a.b[i];
-                const double ri = bi - ax;
-                a.r64[i] = ri;
-                const T rt = cvt<T>(ri);
-                r[i] = rt; rhat[i] = rt; pin[i] = T(0); v[i] = T(0); d[i] = T(0);
-                acc[0] += bi * bi;
-                acc[1] += (double)rt * (double)rt;
-                if (!isfinite(ri)) acc[3] += 1.0;
-                // preconditioner coefficients from the FP64 assembled values
-                double cs = 0.0, cp = 0.0;
-                if (a.precond != kPcNone) {
-                    const uint32_t ds = a.diag_slot[i];
-                    const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
-                    const int pi = a.partner[i];
-                    if (a.precond == kPcAuto && pi >= 0) {
-                        const double akk = a.diag_slot[pi] == kSentinel ? 0.0 : a.vals64[a.diag_slot[pi]];
-                        const double aik = a.vals64[a.off_slot[i]];
-                        const double aki = a.vals64[a.off_slot[pi]];
-                        const double det = aii * akk - aik * aki;
-                        if (fabs(det) > 1e-300) { cs = akk / det; cp = -aik / det; }
-                    } else if (fabs(aii) > 1e-30) {
-                        cs = 1.0 / aii;
-                    } else if (a.precond == kPcAuto) {
-                        cs = 1.0;   // unpaired zero diagonal: identity keeps M^-1 nonsingular
-                    }
-                } else {
-                    cs = 1.0;
-                }
-                pc_self[i] = cvt<T>(cs);
-                pc_part[i] = cvt<T>(cp);
-            });
-            acc[2] = acc[1];
-            double *pr = part();
-            publish_partials<4>(acc, pr, smem);
-            OHM_SYNC();
-            double tot[4];
-            gather_partials<4>(pr, tot, smem);
-            const double bnorm = sqrt(tot[0]);
-            const double r0norm = sqrt(tot[1]);
-            bnorm_last = bnorm;
-            double abs_tol = a.krylov_tol * bnorm;
-            if (a.inner_rtol > 0.0) abs_tol = fmax(abs_tol, a.inner_rtol * r0norm);
-            double rho_new = tot[2];
-            if (a.newton && tot[3] > 0.0) {
-                // non-finite assembled system (newton.rs:258-263)
-                status = kErrNewtonNumerical;
-                err_iter = outer;
-                outer_done = outer;
-                break;
-            }
-
-            const bool linear_done = !a.newton && (r0norm < a.krylov_tol * bnorm || bnorm < 1e-30);
-            if (linear_done) {
-                // converged before this refinement sweep (bicgstab.rs:91-95 for b = 0)
-                kcode = kKrylovConverged;
-                outer_done = outer;
-                final_res = r0norm;
-                break;
-            }
-
-            // ------------------------------ BiCGSTAB ------------------------------
-            double rho = 1.0, alpha = 1.0, omega = 1.0;
-            double rr_cur = tot[1];     // ||r||^2 of the current residual
-            int restarts = 0;
-            kcode = kKrylovRunning;
-            // Restart (r_hat = r, p = v = 0): the shadow residual r_hat = b of
-            // bicgstab.rs:87 is orthogonal to later residuals when b is
-            // supported on a few source rows.  With max_restarts = 0 this is
-            // the reference's breakdown error.
-#define OHM_KRYLOV_RESTART()                                                    \
-    do {                                                                        \
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {               \
-            rhat[i] = r[i]; pin[i] = T(0); v[i] = T(0);                         \
-        }                                                                       \
-        OHM_SYNC();                                                             \
-        rho = 1.0; alpha = 1.0; omega = 1.0; rho_new = rr_cur; ++restarts;      \
-    } while (0)
-            if (!(r0norm < abs_tol)) {
-                int it = 0;
-                for (; it < a.max_krylov; ++it) {
-                    if (fabs(rho_new) < 1e-30) {
-                        if (restarts < a.max_restarts && rr_cur >= 1e-30) {
-                            OHM_KRYLOV_RESTART();
-                        } else {
-                            kcode = kKrylovBreakRho;
-                            break;
-                        }
-                    }
-                    const double beta = (rho_new / rho) * (alpha / omega);
-                    rho = rho_new;
-                    // p = (p - omega v) * beta + r ; phat = M^-1 p
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                        const double pn = ((double)pin[i] + (-omega) * (double)v[i]) * beta + (double)r[i];
-                        const T pt = cvt<T>(pn);
-                        pout[i] = pt;
-                        double z = (double)pc_self[i] * (double)pt;
-                        const int pi = a.partner[i];
-                        if (pi >= 0) {
-                            const T pk = cvt<T>(((double)pin[pi] + (-omega) * (double)v[pi]) * beta + (double)r[pi]);
-                            z += (double)pc_part[i] * (double)pk;
-                        }
-                        phat[i] = cvt<T>(z);
-                    }
-                    { T *tmp = pin; pin = pout; pout = tmp; }
-                    OHM_SYNC();
-                    // v = A phat ; (rhat, v)
-                    double acc1[1] = {0.0};
-                    spmv_rows<LPR>(a.row_ptr, a.col, A, phat, r0, r1, [&](int i, double y) {
-                        const T yt = cvt<T>(y);
-                        v[i] = yt;
-                        acc1[0] += (double)rhat[i] * (double)yt;
-                    });
-                    double *pr_rv = part();
-                    publish_partials<1>(acc1, pr_rv, smem);
-                    OHM_SYNC();
-                    double rv[1];
-                    gather_partials<1>(pr_rv, rv, smem);
-                    if (fabs(rv[0]) < 1e-30) {
-                        if (restarts < a.max_restarts && rr_cur >= 1e-30) {
-                            OHM_KRYLOV_RESTART();
-                            continue;
-                        }
-                        kcode = kKrylovBreakRv;
-                        break;
-                    }
-                    alpha = rho / rv[0];
-                    // s = r - alpha v ; shat = M^-1 s ; ||s||^2
-                    double acc2[1] = {0.0};
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                        const T st = cvt<T>((double)r[i] + (-alpha) * (double)v[i]);
-                        s[i] = st;
-                        acc2[0] += (double)st * (double)st;
-                        double z = (double)pc_self[i] * (double)st;
-                        const int pi = a.partner[i];
-                        if (pi >= 0) {
-                            const T sk = cvt<T>((double)r[pi] + (-alpha) * (double)v[pi]);
-                            z += (double)pc_part[i] * (double)sk;
-                        }
-                        shat[i] = cvt<T>(z);
-                    }
-                    double *pr_ss = part();
-                    publish_partials<1>(acc2, pr_ss, smem);
-                    OHM_SYNC();
-                    double ss[1];
-                    gather_partials<1>(pr_ss, ss, smem);
-                    if (sqrt(ss[0]) < abs_tol) {         // early exit (bicgstab.rs:134-139)
-                        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-                            d[i] = cvt<T>((double)d[i] + alpha * (double)phat[i]);
-                        kcode = kKrylovConverged;
-                        ++it;
-                        break;
-                    }
-                    // t = A shat ; (t, s), (t, t)
-                    double acc3[2] = {0.0, 0.0};
-                    spmv_rows<LPR>(a.row_ptr, a.col, A, shat, r0, r1, [&](int i, double y) {
-                        const T yt = cvt<T>(y);
-                        t[i] = yt;
-                        acc3[0] += (double)yt * (double)s[i];
-                        acc3[1] += (double)yt * (double)yt;
-                    });
-                    double *pr_tt = part();
-                    publish_partials<2>(acc3, pr_tt, smem);
-                    OHM_SYNC();
-                    double tt[2];
-                    gather_partials<2>(pr_tt, tt, smem);
-                    if (fabs(tt[1]) < 1e-30) { kcode = kKrylovBreakTt; break; }
-                    omega = tt[0] / tt[1];
-                    // x += alpha phat ; x += omega shat ; r = s - omega t
-                    double acc4[2] = {0.0, 0.0};
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                        d[i] = cvt<T>(((double)d[i] + alpha * (double)phat[i]) + omega * (double)shat[i]);
-                        const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
-                        r[i] = rt;
-                        acc4[0] += (double)rhat[i] * (double)rt;
-                        acc4[1] += (double)rt * (double)rt;
-                    }
-                    double *pr_rr = part();
-                    publish_partials<2>(acc4, pr_rr, smem);
-                    OHM_SYNC();
-                    double rr[2];
-                    gather_partials<2>(pr_rr, rr, smem);
-                    rho_new = rr[0];
-                    rr_cur = rr[1];
-                    const double rnorm = sqrt(rr[1]);
-                    if (!isfinite(rnorm)) { kcode = kKrylovNan; ++it; break; }
-                    if (rnorm < abs_tol) { kcode = kKrylovConverged; ++it; break; }
-                    if (fabs(omega) < 1e-30) { kcode = kKrylovBreakOmega; ++it; break; }
-                    if (a.accept_partial && it + 1 == a.max_krylov && rnorm < r0norm) {
-                        kcode = kKrylovConverged;   // inexact inner solve accepted (mixed)
-                        ++it;
-                        break;
-                    }
-                }
-#undef OHM_KRYLOV_RESTART
-                if (kcode == kKrylovRunning) kcode = kKrylovMaxIter;
-                kiters += it;
-            } else {
-                kcode = kKrylovConverged;
-            }
-            if (kcode != kKrylovConverged) {
-                status = kErrSolve;
-                err_iter = outer;
-                outer_done = outer;
-                break;
-            }
+            double *pr = g.part();
+            publish_partials<3>(acc, pr, g.smem);
+            OHM_SYNC_OR();
+            gather_partials<3>(pr, acc, g.smem);
+        }
+        const double bnorm = sqrt(acc[0]);
+        const double rnorm64 = sqrt(acc[1]);
+        bnorm_last = bnorm;
+        if (a.newton && acc[2] > 0.0) {
+            // non-finite assembled system (newton.rs:258-263)
+            status = kErrNewtonNumerical;
+            err_iter = outer;
+            outer_done = outer;
+            break;
+        }
+        if (!a.newton && (rnorm64 < a.krylov_tol * bnorm || bnorm < 1e-30)) {
+            // converged before this sweep (bicgstab.rs:91-95 for b = 0)
+            kcode = kKrylovConverged;
+            outer_done = outer;
+            final_res = rnorm64;
+            break;
         }
 
-        // -------------------------------- update --------------------------------
+        // -------------------------------- BiCGSTAB ---------------------------------
+        const double floor_tol = a.krylov_tol * bnorm;
+        KrylovOut ko{0, 0};
+        if (a.mixed) {
+            kcode = krylov<float, LPR>(a, g, floor_tol, a.inner_rtol, true, ko);
+            if (kcode == kKrylovAbort) return;
+            kiters += ko.iterations;
+            restarts += ko.restarts;
+            if (kcode != kKrylovConverged) {
+                ++fallbacks;           // FP32 failed or stalled: redo this solve in FP64
+                kcode = krylov<double, LPR>(a, g, floor_tol, a.inner_rtol, false, ko);
+                if (kcode == kKrylovAbort) return;
+                kiters += ko.iterations;
+                restarts += ko.restarts;
+            }
+        } else {
+            kcode = krylov<double, LPR>(a, g, floor_tol, a.inner_rtol, false, ko);
+            if (kcode == kKrylovAbort) return;
+            kiters += ko.iterations;
+            restarts += ko.restarts;
+        }
+        if (kcode != kKrylovConverged) {
+            status = kErrSolve;
+            err_iter = outer;
+            outer_done = outer;
+            break;
+        }
+
+        // -------------------------------- update ----------------------------------
         if (!a.newton) {
-            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = a.x[i] + (double)d[i];
-            OHM_SYNC();
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = a.x[i] + a.dx[i];
+            OHM_SYNC_OR();
             outer_done = outer + 1;
             continue;      // next refinement sweep recomputes the FP64 residual
         }
         for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
             const double xo = a.x[i];
             a.x_prev[i] = xo;
-            a.x[i] = xo + (double)d[i];
+            a.x[i] = xo + a.dx[i];
             a.node_scale[i] = 0x3FF0000000000000ULL;   // 1.0
         }
-        OHM_SYNC();
+        OHM_SYNC_OR();
         {
             const int ndev = a.nd + a.nq + a.nm;
             for (int k = gtid; k < ndev; k += gstride) {
@@ -441,7 +531,7 @@ __global__ void __launch_bounds__(512) persistent_solver(KernelArgs a) {
                 else mosfet_limit(a.mosfets[k - a.nd - a.nq], a.x_prev, a.x, a.node_scale);
             }
         }
-        OHM_SYNC();
+        OHM_SYNC_OR();
         {
             double mx[3] = {0.0, 0.0, 0.0};   // max|dx|, max|x|, non-finite count
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
@@ -453,50 +543,51 @@ __global__ void __launch_bounds__(512) persistent_solver(KernelArgs a) {
                 mx[0] = fmax(mx[0], fabs(xn - xo));
                 mx[1] = fmax(mx[1], fabs(xn));
             }
-            double *pr = part();
-            publish_max<3>(mx, pr, smem);
-            OHM_SYNC();
-            double g[3];
-            gather_max<3>(pr, g, smem);
-            last_dmax = g[0];
+            double *pr = g.part();
+            publish_max<3>(mx, pr, g.smem);
+            OHM_SYNC_OR();
+            gather_max<3>(pr, mx, g.smem);
+            last_dmax = mx[0];
             outer_done = outer + 1;
-            if (g[2] > 0.0) { status = kErrNewtonNumerical; err_iter = outer; break; }
-            if (g[0] < a.abs_tol + a.rel_tol * g[1]) { status = kOk; break; }
+            if (mx[2] > 0.0) { status = kErrNewtonNumerical; err_iter = outer; break; }
+            if (mx[0] < a.abs_tol + a.rel_tol * mx[1]) { status = kOk; break; }
             if (outer + 1 == a.max_outer) status = kErrNewtonNotConverged;
         }
     }
 
-    // final FP64 residual of a linear solve (reported, and the IR stopping test)
+    // final FP64 residual of a linear solve (reported; the refinement test in mixed mode)
     if (!a.newton && status == kOk && final_res < 0.0) {
         double acc[1] = {0.0};
         spmv_rows<LPR>(a.row_ptr, a.col, a.vals64, a.x, r0, r1, [&](int i, double ax) {
             const double ri = a.b[i] - ax;
             acc[0] += ri * ri;
         });
-        double *pr = part();
-        publish_partials<1>(acc, pr, smem);
-        OHM_SYNC();
-        double rr[1];
-        gather_partials<1>(pr, rr, smem);
-        final_res = sqrt(rr[0]);
+        double *pr = g.part();
+        publish_partials<1>(acc, pr, g.smem);
+        OHM_SYNC_OR();
+        gather_partials<1>(pr, acc, g.smem);
+        final_res = sqrt(acc[0]);
         if (a.require_true_residual && !(final_res < a.krylov_tol * bnorm_last)) {
             // refinement sweeps exhausted without reaching the FP64 tolerance
             status = kErrSolve;
             if (kcode == kKrylovConverged) kcode = kKrylovMaxIter;
         }
     }
-#undef OHM_SYNC
 
-    if (bid == 0 && threadIdx.x == 0) {
+    if (g.bid == 0 && threadIdx.x == 0) {
         a.info->status = status;
         a.info->krylov_code = kcode;
         a.info->iterations = outer_done;
         a.info->error_iteration = err_iter;
         a.info->krylov_iterations = kiters;
+        a.info->fp64_fallbacks = fallbacks;
+        a.info->krylov_restarts = restarts;
         a.info->max_residual = last_dmax;
         a.info->final_residual = final_res;
         a.info->b_norm = bnorm_last;
     }
 }
+
+#undef OHM_SYNC_OR
 
 }  // namespace ohm

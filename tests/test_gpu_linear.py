@@ -87,11 +87,14 @@ def _rel_err(x, ref, sl):
 
 @pytest.mark.parametrize("n_nodes", [200, 2000])
 def test_ladder_fp64_vs_dense_oracle(ctx, n_nodes):
-    """Resistor ladder (the 10k-node benchmark recipe, smaller): Jacobi
-    BiCGSTAB at tol 1e-12 vs the dense GE restatement, 1e-9 norm-wise."""
+    """Resistor ladder (the 10k-node benchmark recipe, smaller): block-Jacobi
+    BiCGSTAB vs the dense GE restatement, 1e-9 norm-wise.  The residual
+    tolerance is relative to ||b|| = the 10 V source, so the node-current
+    residual of tol 1e-12 still leaves ~2e-9 relative voltage error on this
+    ladder; 1e-13 meets the 1e-9 bar."""
     s = mna.compile_circuit(ck.resistor_ladder(n_nodes, seed=0))
     ref = linear_ref.dense_solve_real(s.size, s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
-    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-12))
+    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-13))
     x = solver.solve_real(s.g, s.b_dc)
     assert _rel_err(x, ref, slice(0, s.n_nodes)) < 1e-9
     assert _rel_err(x, ref, slice(s.n_nodes, s.size)) < 1e-9
@@ -102,19 +105,22 @@ def test_ladder_10k_fp64_and_mixed(ctx):
     s = mna.compile_circuit(ck.resistor_ladder(10_000, seed=0))
     ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
     for prec in (0, 1):
-        p = S.BiCgStabParams(tolerance=1e-12, precision=prec, max_refinements=30, max_iterations=20000)
+        p = S.BiCgStabParams(tolerance=1e-13, precision=prec, max_refinements=30, max_iterations=20000)
         x = S.GpuSolver(ctx, p).solve_real(s.g, s.b_dc)
         assert _rel_err(x, ref, slice(0, s.n_nodes)) < 1e-9, prec
         assert _rel_err(x, ref, slice(s.n_nodes, s.size)) < 1e-9, prec
 
 
 def test_mixed_precision_iterative_refinement(ctx):
-    s = mna.compile_circuit(ck.diode_mesh(30, 30, seed=11, diode_frac=0.0))
+    """FP32 Krylov inside FP64 iterative refinement reaches the FP64 answer."""
+    s = mna.compile_circuit(ck.resistor_ladder(2000, seed=4))
     ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
-    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-12, precision=1, max_refinements=20))
+    solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-14, precision=1, max_refinements=20))
     x = solver.solve_real(s.g, s.b_dc)
-    assert _rel_err(x, ref, slice(0, s.size)) < 1e-9
+    assert _rel_err(x, ref, slice(0, s.n_nodes)) < 1e-9
+    assert _rel_err(x, ref, slice(s.n_nodes, s.size)) < 1e-9
     assert solver.last_info["iterations"] >= 2        # refinement sweeps were used
+    assert solver.last_info["final_residual_norm"] < 1e-14 * solver.last_info["b_norm"]
 
 
 def test_backend_ops(ctx):
