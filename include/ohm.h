@@ -173,6 +173,23 @@ ohm_status ohm_solve_real(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *
 ohm_status ohm_solve_real_device(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *b, ohm_buf *x,
                                  const ohm_krylov_params *params, ohm_solve_info *info);
 
+/* The solve of ohm_solve_real for callers that cannot allocate device memory
+ * (no counterpart in the reference).  Some callers run inside another
+ * program's device-memory budget, or on a path where cudaMalloc/cudaFree would
+ * synchronise the device or fail under memory pressure; this entry point
+ * calls neither.  The caller passes device pointers for the CSR, b and the
+ * output x, and the stream to run on (NULL = the default stream), on the
+ * current device.  All other working memory is one fixed file-scope device
+ * array of about 5.4 MB, held by every GPU that loads the library until the
+ * process exits; systems above 32768 rows or 262144 nonzeros are rejected
+ * with OHM_ERR_INVALID_ARG.  The first call on a device looks up that
+ * device's address of the array: make it before any stream capture.  Every
+ * call shares the array, so calls that overlap on the GPU race; x and all
+ * state that must start at zero are cleared by each call. */
+ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nnz, const uint32_t *d_row_ptr,
+                                  const uint32_t *d_col, const double *d_values, const double *d_b,
+                                  double *d_x, const ohm_krylov_params *params, ohm_solve_info *info);
+
 /* ---- newton_solve (src/solver/newton.rs:65-78) ---------------------------
  * Argument order follows the reference.  x_out receives the solution
  * (size entries).  The whole Newton loop (evaluate, stamp, solve, limit,

@@ -74,6 +74,8 @@ SIGNATURES = {
                                  C.POINTER(KrylovParams), C.POINTER(SolveInfo)]),
     "ohm_solve_real_device": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(KrylovParams),
                                         C.POINTER(SolveInfo)]),
+    "ohm_solve_real_noalloc": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp,
+                                         C.POINTER(KrylovParams), C.POINTER(SolveInfo)]),
     "ohm_newton_solve": (C.c_int, [_vp, _dp, _u32p, _u32p, _dp, _vp, _i64, _vp, _i64, _vp, _i64,
                                    _i64, _i64, C.POINTER(NewtonParamsC), _dp, C.POINTER(SolveInfo)]),
     "ohm_plan_create": (C.c_int, [_vp, _dp, _u32p, _u32p, _dp, _vp, _i64, _vp, _i64, _vp, _i64, _dp,

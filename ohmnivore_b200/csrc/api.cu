@@ -249,7 +249,7 @@ static int choose_lpr(int64_t n, int64_t nnz) {
 
 static constexpr int kBlock = 512;
 
-static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, int64_t nnz, int *launches) {
+ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t nnz, int *launches) {
     const int lpr = choose_lpr(a.n, nnz);
     KernelFn fn = pick_kernel(lpr);
     int per_sm = 0;
@@ -259,25 +259,39 @@ static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, int64_t nnz, int *lau
     int64_t want = (a.n + kBlock - 1) / kBlock;
     const int64_t ndev = (int64_t)a.nd + a.nq + a.nm;
     want = std::max<int64_t>(want, (ndev + kBlock - 1) / kBlock);
-    int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
-    a.gs.count = c->sync_words;
-    a.gs.gen = c->sync_words + 1;
-    a.gs.error = (int *)(c->sync_words + 2);
-    a.info = c->info_dev;
-    CUDA_TRY(cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream));
-    CUDA_TRY(cudaMemsetAsync(c->info_dev, 0, sizeof(DeviceInfo), c->stream));
+    int64_t cap = (int64_t)per_sm * t.num_sms;
+    if (t.max_grid > 0) cap = std::min<int64_t>(cap, t.max_grid);
+    int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+    a.gs.count = t.sync_words;
+    a.gs.gen = t.sync_words + 1;
+    a.gs.error = (int *)(t.sync_words + 2);
+    a.info = t.info_dev;
+    CUDA_TRY(cudaMemsetAsync(t.sync_words, 0, 4 * sizeof(unsigned int), t.stream));
+    CUDA_TRY(cudaMemsetAsync(t.info_dev, 0, sizeof(DeviceInfo), t.stream));
     void *args[] = {&a};
-    CUDA_TRY(cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kBlock), args, 0, c->stream));
+    CUDA_TRY(cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kBlock), args, 0, t.stream));
     if (launches) *launches += 1;
     return OHM_OK;
 }
 
+static LaunchTarget ctx_target(ohm_ctx *c) {
+    return LaunchTarget{c->num_sms, c->stream, c->sync_words, c->info_dev, c->info_host, 0};
+}
+
+static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, int64_t nnz, int *launches) {
+    return ohm_launch_persistent(ctx_target(c), a, nnz, launches);
+}
+
 static ohm_status finish_solver(ohm_ctx *c, ohm_solve_info *info, int launches) {
+    return ohm_finish_persistent(ctx_target(c), info, launches);
+}
+
+ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, int launches) {
     unsigned int words[4] = {0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpyAsync(c->info_host, c->info_dev, sizeof(DeviceInfo), cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
-    const DeviceInfo &di = *c->info_host;
+    CUDA_TRY(cudaMemcpyAsync(t.info_host, t.info_dev, sizeof(DeviceInfo), cudaMemcpyDeviceToHost, t.stream));
+    CUDA_TRY(cudaMemcpyAsync(words, t.sync_words, sizeof words, cudaMemcpyDeviceToHost, t.stream));
+    CUDA_TRY(cudaStreamSynchronize(t.stream));
+    const DeviceInfo &di = *t.info_host;
     ohm_status st = OHM_OK;
     if (words[2] != 0) {
         st = fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
@@ -367,7 +381,7 @@ struct Workspace {
     }
 };
 
-static ohm_status check_krylov(const ohm_krylov_params *p) {
+ohm_status ohm_check_krylov(const ohm_krylov_params *p) {
     if (!p) return fail(OHM_ERR_INVALID_ARG, "params is null");
     if (p->max_iterations <= 0) return fail(OHM_ERR_SOLVE, "BiCGSTAB max_iterations must be > 0");
     if (!(p->tolerance > 0.0) || !std::isfinite(p->tolerance))
@@ -384,6 +398,12 @@ static ohm_status check_krylov(const ohm_krylov_params *p) {
 __global__ void f64_to_f32_kernel(const double *in, float *out, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (float)in[i];
+}
+
+cudaError_t ohm_f64_to_f32(const double *in, float *out, int64_t n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096)), 256, 0, s>>>(in, out, n);
+    return cudaGetLastError();
 }
 
 // -------------------------------------------------------- linear solves --
@@ -433,7 +453,7 @@ extern "C" ohm_status ohm_solve_real(ohm_ctx *c, int64_t n, int64_t nnz, const u
                                      const double *values, const double *b, double *x, const ohm_krylov_params *params,
                                      ohm_solve_info *info) {
     if (!c) return fail(OHM_ERR_INVALID_ARG, "ctx is null");
-    ohm_status st = check_krylov(params);
+    ohm_status st = ohm_check_krylov(params);
     if (st != OHM_OK) return st;
     if (n == 0) return OHM_OK;                       // cpu.rs:39-41, gpu.rs:118-120
     if (!b || !x || (nnz && !values)) return fail(OHM_ERR_INVALID_ARG, "null array");
@@ -682,7 +702,7 @@ static ohm_status check_newton(const ohm_newton_params *np) {
     if (np->max_iterations <= 0)
         return fail(OHM_ERR_NEWTON_NOT_CONVERGED, "Newton solver did not converge after 0 iterations");
     if (!(np->abs_tol >= 0.0) || !(np->rel_tol >= 0.0)) return fail(OHM_ERR_INVALID_ARG, "negative tolerance");
-    return check_krylov(&np->krylov);
+    return ohm_check_krylov(&np->krylov);
 }
 
 extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const ohm_newton_params *np,
@@ -732,7 +752,7 @@ extern "C" ohm_status ohm_newton_solve(ohm_ctx *c, const double *base_g_values, 
 extern "C" ohm_status ohm_solve_real_device(ohm_ctx *c, const ohm_csr *a, const ohm_buf *b, ohm_buf *x,
                                             const ohm_krylov_params *params, ohm_solve_info *info) {
     if (!c || !a || !b || !x) return fail(OHM_ERR_INVALID_ARG, "null argument");
-    ohm_status st = check_krylov(params);
+    ohm_status st = ohm_check_krylov(params);
     if (st != OHM_OK) return st;
     if (b->n != a->n || x->n != a->n) return fail(OHM_ERR_INVALID_ARG, "dimension mismatch");
     if (a->n == 0) return OHM_OK;

@@ -38,6 +38,20 @@ struct ohm_ctx {
     bool destroy_pending = false;
 };
 
+// Where a persistent-solver launch puts its barrier words and status block.
+struct LaunchTarget {
+    int num_sms;
+    cudaStream_t stream;
+    unsigned int *sync_words;        // 4 words: count, generation, error, spare
+    ohm::DeviceInfo *info_dev;
+    ohm::DeviceInfo *info_host;      // host copy target (pinned or not)
+    int max_grid;                    // 0: no cap beyond the co-residency limit
+};
+ohm_status ohm_launch_persistent(const LaunchTarget &t, ohm::KernelArgs &a, int64_t nnz, int *launches);
+ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, int launches);
+ohm_status ohm_check_krylov(const ohm_krylov_params *p);
+cudaError_t ohm_f64_to_f32(const double *in, float *out, int64_t n, cudaStream_t s);
+
 // Child-object bookkeeping (see ohm_ctx::live_objects).
 void ohm_ctx_retain(ohm_ctx *c);
 void ohm_ctx_release(ohm_ctx *c);
