@@ -50,9 +50,13 @@ def parse():
 
 
 def newton_params(mixed: bool):
+    """Newton stops at max|dx| < 1e-9 V; each linear solve is inexact with an
+    Eisenstat-Walker tolerance in [1e-4, 0.1] above an absolute floor of
+    1e-14 ||b||.  The same settings for the FP64 and the mixed path."""
     from ohmnivore_b200 import solver as S
-    return S.NewtonParams(max_iterations=100, abs_tol=1e-10, bicgstab_max_iterations=20000,
-                          bicgstab_tolerance=1e-14, precision=1 if mixed else 0, inner_rtol=1e-4)
+    return S.NewtonParams(max_iterations=200, abs_tol=1e-9, bicgstab_max_iterations=20000,
+                          bicgstab_tolerance=1e-14, precision=1 if mixed else 0, inner_rtol=1e-4,
+                          forcing=1, eta_max=0.1)
 
 
 class ClockSampler:
@@ -236,11 +240,12 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item()), infos, x.cpu().numpy()
 
-    # ---- mixed precision (headline) and plain FP64, device-resident ----
+    # ---- FP64 path (headline: faster on this latency-bound single circuit)
+    #      and the mixed-precision path, both device-resident ----
     with ClockSampler(local_rank) as clk:
-        mixed_ms, mixed_infos, x_mixed = timed_solves(True, args.steps, args.warmup)
+        fp64_ms, fp64_infos, x_fp64 = timed_solves(False, args.steps, args.warmup)
     clocks = clk.summary()
-    fp64_ms, fp64_infos, x_fp64 = timed_solves(False, args.steps, args.warmup)
+    mixed_ms, mixed_infos, x_mixed = timed_solves(True, args.steps, args.warmup)
 
     # ---- e2e: public C ABI, pinned host arrays, upload + solve + download ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -250,7 +255,7 @@ def main():
     h_b = pin(sysm.b_dc.astype(np.float64))
     h_dd = torch.from_numpy(sysm.diode_descriptors.view(np.uint8)).pin_memory().numpy().view(mna.DIODE_DTYPE)
     h_x = pin(np.zeros(n))
-    params = newton_params(True)
+    params = newton_params(False)
 
     def e2e_call():
         return S.newton_solve(ctx, h_vals, h_col, h_rp, h_b, h_dd, sysm.bjt_descriptors,
@@ -286,35 +291,39 @@ def main():
     peaks = measured_peaks()
     hbm_peak = peaks["hbm_gbs"] if peaks else 6650.0
     peak_src = "measured" if peaks else "fallback"
-    info0 = mixed_infos[-1]
-    algo_bytes, kry = solve_bytes(info0, n, nnz, nd, mixed=True)
-    per_launch_ms = mixed_ms / args.steps
+    info0 = fp64_infos[-1]
+    algo_bytes, kry = solve_bytes(info0, n, nnz, nd, mixed=False)
+    per_launch_ms = fp64_ms / args.steps
     achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
 
-    value = world * args.steps / (mixed_ms * 1e-3)
-    fp64_value = world * args.steps / (fp64_ms * 1e-3)
+    value = world * args.steps / (fp64_ms * 1e-3)
+    mixed_value = world * args.steps / (mixed_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": mixed_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 Krylov / f64 Newton", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "mixed (FP32 BiCGSTAB bulk, FP64 eval/residual/update)",
+        "warmup": args.warmup, "ms_per_step": fp64_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "FP64 (BiCGSTAB, device eval, residual, update)",
                    "preconditioner": "block Jacobi (2x2 for the source branch row)",
-                   "newton_abs_tol": 1e-10, "krylov_tol_floor": 1e-14, "inner_rtol": 1e-4,
+                   "newton_abs_tol": 1e-9, "krylov_tol_floor": 1e-14,
+                   "inner_tolerance": "Eisenstat-Walker in [1e-4, 0.1]",
                    "l2": "flushed (512 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-        "plain_fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": fp64_ms / args.steps,
-                       "newton_iterations": fp64_infos[-1]["iterations"],
-                       "krylov_iterations": fp64_infos[-1]["krylov_iterations"]},
-        "mixed_vs_fp64": value / fp64_value,
+        "mixed_precision": {"value": mixed_value, "unit": "solves/s", "ms_per_step": mixed_ms / args.steps,
+                            "newton_iterations": mixed_infos[-1]["iterations"],
+                            "krylov_iterations": mixed_infos[-1]["krylov_iterations"],
+                            "fp64_fallbacks": mixed_infos[-1]["fp64_fallbacks"],
+                            "note": "FP32 BiCGSTAB bulk; on this single L2-resident circuit the loop is "
+                                    "latency-bound, so FP32 iterations cost the same as FP64 ones"},
+        "mixed_vs_fp64": mixed_value / value,
         "newton_iterations": info0["iterations"], "krylov_iterations": kry,
-        "fp64_fallbacks": info0["fp64_fallbacks"], "krylov_restarts": info0["krylov_restarts"],
+        "krylov_restarts": info0["krylov_restarts"],
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "api": "ohm_newton_solve (host arrays in pinned memory)"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                     "kernel": "persistent_solver<float,2>",
+                     "kernel": "persistent_solver<2> (FP64 Krylov)",
                      "algorithmic_bytes_per_launch": algo_bytes,
                      "note": "working set (~40 MB) is L2-resident inside a solve"},
         "spmv": spmv,
@@ -333,7 +342,7 @@ def main():
         line["rel_err_vs_oracle"] = {
             "mixed": {"voltages": err(x_mixed, nn), "currents": err(x_mixed, br)},
             "fp64": {"voltages": err(x_fp64, nn), "currents": err(x_fp64, br)},
-            "e2e_mixed": {"voltages": err(h_x, nn), "currents": err(h_x, br)}}
+            "e2e_fp64": {"voltages": err(h_x, nn), "currents": err(h_x, br)}}
         line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
                                 "sample": f"1 full DC solve of the workload ({it_ref} FP64 Newton "
                                           "iterations, SuperLU per iteration), single thread"}

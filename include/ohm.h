@@ -99,7 +99,15 @@ typedef struct {                 /* BiCgStabParams (src/solver/bicgstab.rs:14-27
                                     > 1 also requires the FP64 residual to meet the tolerance */
     int32_t max_restarts;        /* restarts with r_hat = r after a rho or r_hat.v breakdown;
                                     0 = the reference's breakdown error; default 50 */
+    int32_t fp32_max_iterations; /* mixed: iterations of an FP32 attempt before the solve is
+                                    redone in FP64 (unless it reduced ||r|| by 2x); default 600 */
+    int32_t reserved;
 } ohm_krylov_params;
+
+typedef enum {
+    OHM_FORCING_CONSTANT = 0,    /* inner tolerance = krylov.inner_rtol */
+    OHM_FORCING_EW = 1           /* Eisenstat-Walker (choice 2), floor krylov.inner_rtol */
+} ohm_forcing;
 
 typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + extensions */
     int32_t max_iterations;      /* default 50 */
@@ -107,6 +115,8 @@ typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + 
     double rel_tol;              /* extension, default 0 */
     ohm_krylov_params krylov;    /* linear sub-solve; reference default tolerance 1e-5 */
     const double *initial_guess; /* NewtonParams::initial_guess, host pointer, may be NULL */
+    int32_t forcing;             /* ohm_forcing, default constant */
+    double eta_max;              /* Eisenstat-Walker upper bound, default 0.5 */
 } ohm_newton_params;
 
 typedef struct {
@@ -180,7 +190,7 @@ ohm_status ohm_solve_real_device(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *
  * calls neither.  The caller passes device pointers for the CSR, b and the
  * output x, and the stream to run on (NULL = the default stream), on the
  * current device.  All other working memory is one fixed file-scope device
- * array of about 5.4 MB, held by every GPU that loads the library until the
+ * array of about 6.2 MB, held by every GPU that loads the library until the
  * process exits; systems above 32768 rows or 262144 nonzeros are rejected
  * with OHM_ERR_INVALID_ARG.  The first call on a device looks up that
  * device's address of the array: make it before any stream capture.  Every
@@ -218,6 +228,12 @@ ohm_status ohm_plan_set_base(ohm_plan *plan, const double *base_g_values, const 
  * receiving the solution. */
 ohm_status ohm_plan_newton_device(ohm_plan *plan, double *x_inout_device,
                                   const ohm_newton_params *params, ohm_solve_info *info);
+/* Per-Newton-iteration record of the last ohm_plan_newton_device call, 6
+ * doubles per iteration: FP32 Krylov iterations, FP64 Krylov iterations,
+ * ||b - J x|| before the solve, inner tolerance, max|x - x_old|, restarts
+ * (rows after the last iteration are NaN).  Stats::bicgstab_iters_per_newton
+ * (src/stats.rs) is the reference counterpart. */
+ohm_status ohm_plan_trace(ohm_plan *plan, double *out, int32_t max_rows, int32_t *rows);
 /* Device-side system matrix / rhs of the last assembly (for tests). */
 ohm_status ohm_plan_download_system(ohm_plan *plan, double *values, double *rhs);
 /* Evaluate + stamp at x (host), return J values and b_eq (host): one assembly. */

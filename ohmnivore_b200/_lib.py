@@ -23,12 +23,14 @@ PRECOND_AUTO, PRECOND_JACOBI, PRECOND_ISAI1, PRECOND_NONE = 0, 1, 2, 3
 class KrylovParams(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("tolerance", C.c_double), ("precision", C.c_int32),
                 ("precond", C.c_int32), ("inner_rtol", C.c_double), ("max_refinements", C.c_int32),
-                ("max_restarts", C.c_int32)]
+                ("max_restarts", C.c_int32), ("fp32_max_iterations", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class NewtonParamsC(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
-                ("krylov", KrylovParams), ("initial_guess", C.POINTER(C.c_double))]
+                ("krylov", KrylovParams), ("initial_guess", C.POINTER(C.c_double)),
+                ("forcing", C.c_int32), ("eta_max", C.c_double)]
 
 
 class SolveInfo(C.Structure):
@@ -86,6 +88,7 @@ SIGNATURES = {
     "ohm_plan_download_system": (C.c_int, [_vp, _dp, _dp]),
     "ohm_plan_assemble": (C.c_int, [_vp, _dp, _dp, _dp]),
     "ohm_plan_limit": (C.c_int, [_vp, _dp, _dp]),
+    "ohm_plan_trace": (C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int32)]),
 }
 
 _LIB = None

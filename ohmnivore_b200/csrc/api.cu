@@ -47,6 +47,8 @@ extern "C" void ohm_krylov_params_default(ohm_krylov_params *p) {
     p->inner_rtol = 0.0;
     p->max_refinements = 1;
     p->max_restarts = 50;
+    p->fp32_max_iterations = 600;
+    p->reserved = 0;
 }
 
 extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
@@ -56,6 +58,8 @@ extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
     p->rel_tol = 0.0;
     ohm_krylov_params_default(&p->krylov);
     p->initial_guess = nullptr;
+    p->forcing = OHM_FORCING_CONSTANT;
+    p->eta_max = 0.5;
 }
 
 // ---------------------------------------------------------------- context --
@@ -178,6 +182,8 @@ static ohm_status check_devices(const ohm_diode_desc *d, int64_t nd, const ohm_b
 struct PcHost {
     std::vector<int32_t> partner;
     std::vector<uint32_t> diag_slot, off_slot;
+    std::vector<uint8_t> rowflag;   // row or one of its columns is paired
+    bool any_pair = false;
 };
 
 static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, const double *val,
@@ -185,10 +191,15 @@ static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, co
     pc.partner.assign(n, -1);
     pc.diag_slot.assign(n, kSentinel);
     pc.off_slot.assign(n, kSentinel);
+    pc.rowflag.clear();
+    pc.any_pair = false;
     for (int64_t i = 0; i < n; ++i)
         for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
             if ((int64_t)col[k] == i) { pc.diag_slot[i] = k; break; }
-    if (!pairs) return;
+    if (!pairs) {
+        pc.rowflag.assign(n, 0);
+        return;
+    }
     auto zero_diag = [&](int64_t i) {
         const uint32_t s = pc.diag_slot[i];
         if (s == kSentinel) return true;
@@ -219,8 +230,16 @@ static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, co
             pc.partner[best] = (int32_t)k;
             pc.off_slot[k] = best_kj;
             pc.off_slot[best] = best_jk;
+            pc.any_pair = true;
         }
     }
+    pc.rowflag.assign(n, 0);
+    if (pc.any_pair)
+        for (int64_t i = 0; i < n; ++i) {
+            bool f = pc.partner[i] >= 0;
+            for (uint32_t k = rp[i]; k < rp[i + 1] && !f; ++k) f = pc.partner[col[k]] >= 0;
+            pc.rowflag[i] = f ? 1 : 0;
+        }
 }
 
 // ------------------------------------------------------------ launch logic --
@@ -247,7 +266,7 @@ static int choose_lpr(int64_t n, int64_t nnz) {
     return 32;
 }
 
-static constexpr int kBlock = 512;
+static constexpr int kBlock = kSolverBlock;
 
 ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t nnz, int *launches) {
     const int lpr = choose_lpr(a.n, nnz);
@@ -262,9 +281,8 @@ ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t n
     int64_t cap = (int64_t)per_sm * t.num_sms;
     if (t.max_grid > 0) cap = std::min<int64_t>(cap, t.max_grid);
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
-    a.gs.count = t.sync_words;
-    a.gs.gen = t.sync_words + 1;
-    a.gs.error = (int *)(t.sync_words + 2);
+    a.gs.count = (unsigned long long *)t.sync_words;     // words 0-1
+    a.gs.error = (int *)(t.sync_words + 2);              // word 2
     a.info = t.info_dev;
     CUDA_TRY(cudaMemsetAsync(t.sync_words, 0, 4 * sizeof(unsigned int), t.stream));
     CUDA_TRY(cudaMemsetAsync(t.info_dev, 0, sizeof(DeviceInfo), t.stream));
@@ -335,48 +353,58 @@ ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, in
     return st;
 }
 
-// Krylov workspace shared by the linear solve and the Newton plan: ten
-// vectors of 8-byte slots (large enough for either precision), the FP64
-// residual, preconditioner coefficients, and the reduction partials.
+// Krylov workspace shared by the linear solve and the Newton plan: two
+// record arrays (4 values per row, 8-byte slots so either precision fits),
+// seven length-n vectors, the FP64 residual and correction, the
+// preconditioner structure and the reduction partials.
 struct Workspace {
     int64_t n = 0;
-    double *vec = nullptr;       // 12 * n doubles
+    double *vec = nullptr;       // 15 * n doubles
     double *r64 = nullptr;
     double *dx = nullptr;
     double *partials = nullptr;  // 8 * max grid
     int32_t *partner = nullptr;
     uint32_t *diag_slot = nullptr, *off_slot = nullptr;
+    uint8_t *rowflag = nullptr;
+    bool any_pair = false;
     void release() {
         cudaFree(vec); cudaFree(r64); cudaFree(dx); cudaFree(partials);
-        cudaFree(partner); cudaFree(diag_slot); cudaFree(off_slot);
+        cudaFree(partner); cudaFree(diag_slot); cudaFree(off_slot); cudaFree(rowflag);
         vec = r64 = dx = partials = nullptr; partner = nullptr; diag_slot = off_slot = nullptr;
+        rowflag = nullptr;
     }
     cudaError_t alloc(int64_t n_, int num_sms) {
         n = n_;
-        cudaError_t e = dalloc(&vec, 12 * (size_t)n);
+        cudaError_t e = dalloc(&vec, 15 * (size_t)n);
         if (e == cudaSuccess) e = dalloc(&r64, n);
         if (e == cudaSuccess) e = dalloc(&dx, n);
         if (e == cudaSuccess) e = dalloc(&partials, 8 * (size_t)num_sms * 8);
         if (e == cudaSuccess) e = dalloc(&partner, n);
         if (e == cudaSuccess) e = dalloc(&diag_slot, n);
         if (e == cudaSuccess) e = dalloc(&off_slot, n);
+        if (e == cudaSuccess) e = dalloc(&rowflag, n);
         return e;
     }
     void bind(KernelArgs &a) const {
-        void **slots[] = {&a.r, &a.rhat, &a.p0, &a.p1, &a.v, &a.s, &a.t, &a.phat, &a.shat, &a.d,
-                          &a.pc_self, &a.pc_part};
-        for (int k = 0; k < 12; ++k) *slots[k] = (void *)(vec + (size_t)k * n);
+        a.rec0 = (void *)vec;
+        a.rec1 = (void *)(vec + 4 * (size_t)n);
+        void **slots[] = {&a.rhat, &a.s, &a.t, &a.phat, &a.shat, &a.d, &a.pc_part};
+        for (int k = 0; k < 7; ++k) *slots[k] = (void *)(vec + (8 + (size_t)k) * n);
         a.r64 = r64;
         a.dx = dx;
         a.partials = partials;
         a.partner = partner;
         a.diag_slot = diag_slot;
         a.off_slot = off_slot;
+        a.rowflag = any_pair ? rowflag : nullptr;
     }
     cudaError_t upload_pc(const PcHost &pc, cudaStream_t s) {
         cudaError_t e = cudaMemcpyAsync(partner, pc.partner.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(diag_slot, pc.diag_slot.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(off_slot, pc.off_slot.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rowflag, pc.rowflag.data(), n * sizeof(uint8_t), cudaMemcpyHostToDevice, s);
+        // the host vectors must outlive the copies: callers synchronise before releasing them
+        any_pair = pc.any_pair;
         return e;
     }
 };
@@ -441,6 +469,8 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     a.inner_rtol = mixed ? (p->inner_rtol > 0.0 ? p->inner_rtol : 1e-4) : p->inner_rtol;
     a.require_true_residual = p->max_refinements > 1 ? 1 : 0;
     a.max_restarts = std::max(0, p->max_restarts);
+    a.fp32_max_iterations = p->fp32_max_iterations > 0 ? p->fp32_max_iterations : p->max_iterations;
+    a.eta_max = 0.5;
     st = launch_solver(c, a, nnz, &launches);
     if (st == OHM_OK) st = finish_solver(c, info, launches);
     cudaStreamSynchronize(c->stream);
@@ -485,6 +515,7 @@ extern "C" ohm_status ohm_solve_real(ohm_ctx *c, int64_t n, int64_t nnz, const u
 }
 
 // ------------------------------------------------------------ Newton plan --
+static constexpr int kTraceRows = 256;
 struct ohm_plan {
     ohm_ctx *ctx = nullptr;
     int64_t n = 0, nnz = 0, nd = 0, nq = 0, nm = 0;
@@ -501,6 +532,7 @@ struct ohm_plan {
     uint32_t *mslot = nullptr, *mslot_ptr = nullptr, *mslot_ids = nullptr;
     uint32_t *rrow = nullptr, *rrow_ptr = nullptr, *rrow_ids = nullptr;
     unsigned long long *node_scale = nullptr;
+    double *trace = nullptr;           // kTraceRows x kTraceCols
     Workspace ws;
     // host copies needed to rebuild the preconditioner when the base changes
     std::vector<uint32_t> h_rp, h_col;
@@ -518,6 +550,7 @@ static void plan_free(ohm_plan *p) {
     cudaFree(p->mslot); cudaFree(p->mslot_ptr); cudaFree(p->mslot_ids);
     cudaFree(p->rrow); cudaFree(p->rrow_ptr); cudaFree(p->rrow_ids);
     cudaFree(p->node_scale);
+    cudaFree(p->trace);
     p->ws.release();
     delete p;
 }
@@ -617,6 +650,7 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     if (e == cudaSuccess) e = up(&p->rrow_ptr, rptr.data(), rptr.size(), s);
     if (e == cudaSuccess) e = up(&p->rrow_ids, rids.data(), rids.size(), s);
     if (e == cudaSuccess) e = dalloc(&p->node_scale, size);
+    if (e == cudaSuccess) e = dalloc(&p->trace, (size_t)kTraceRows * kTraceCols);
     if (e == cudaSuccess) e = p->ws.alloc(size, c->num_sms);
     if (e == cudaSuccess && nnz) {
         f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, nnz);
@@ -662,6 +696,19 @@ extern "C" ohm_status ohm_plan_set_base(ohm_plan *p, const double *base_g_values
     return OHM_OK;
 }
 
+static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, KernelArgs &a);
+
+extern "C" ohm_status ohm_plan_trace(ohm_plan *p, double *out, int32_t max_rows, int32_t *rows) {
+    if (!p || !out || max_rows < 0) return fail(OHM_ERR_INVALID_ARG, "bad trace arguments");
+    const int r = std::min<int>(max_rows, kTraceRows);
+    if (r > 0)
+        CUDA_TRY(cudaMemcpyAsync(out, p->trace, (size_t)r * kTraceCols * sizeof(double), cudaMemcpyDeviceToHost,
+                                 p->ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+    if (rows) *rows = r;
+    return OHM_OK;
+}
+
 static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, KernelArgs &a) {
     const ohm_krylov_params &kp = np->krylov;
     const int want_pc = kp.precond == OHM_PRECOND_AUTO ? 1 : 0;
@@ -694,6 +741,11 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.mixed = mixed ? 1 : 0;
     a.inner_rtol = mixed ? (kp.inner_rtol > 0.0 ? kp.inner_rtol : 1e-4) : kp.inner_rtol;
     a.max_restarts = std::max(0, kp.max_restarts);
+    a.fp32_max_iterations = kp.fp32_max_iterations > 0 ? kp.fp32_max_iterations : kp.max_iterations;
+    a.forcing = np->forcing;
+    a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
+    a.trace = p->trace;
+    a.trace_cap = kTraceRows;
     return OHM_OK;
 }
 
@@ -717,6 +769,7 @@ extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const o
     KernelArgs a;
     st = plan_args(p, np, x_dev, a);
     if (st != OHM_OK) return st;
+    CUDA_TRY(cudaMemsetAsync(p->trace, 0xFF, (size_t)kTraceRows * kTraceCols * sizeof(double), c->stream));
     int launches = 0;
     st = launch_solver(c, a, p->nnz, &launches);
     if (st != OHM_OK) return st;

@@ -13,47 +13,51 @@ constexpr uint32_t kSentinel = 0xFFFFFFFFu;   // u32::MAX, ground / absent slot
 constexpr int kStatusOk = 0;
 constexpr int kStatusTimeout = 5;
 
-// Upper bound on one barrier wait: iterations of a __nanosleep(128) loop
-// (about 2^24 * 128 ns = 2 s).  A wait that runs out records kStatusTimeout
-// and the kernel returns; with a cooperative launch every block is resident,
-// so a healthy barrier never comes near the bound.
-constexpr uint32_t kBarrierSpinLimit = 1u << 24;
+// Upper bound on one barrier wait: spin iterations (tight for the first
+// kTightSpins, then __nanosleep(64)); about 2-3 s in total.  A wait that runs
+// out records kStatusTimeout and the kernel returns; with a cooperative launch
+// every block is resident, so a healthy barrier never comes near the bound.
+constexpr uint32_t kBarrierSpinLimit = 1u << 22;
+constexpr uint32_t kTightSpins = 2048;
 
 struct GridSync {
-    unsigned int *count;   // arrivals in the current generation
-    unsigned int *gen;     // generation counter
-    int *error;            // first error recorded by any block (0 = none)
+    unsigned long long *count;   // arrivals since launch (monotone, zeroed per launch)
+    int *error;                  // first error recorded by any block (0 = none)
 };
 
-// Grid-wide barrier for co-resident (cooperatively launched) blocks.
-// Returns false when the wait gave up or another block recorded an error;
-// the caller must then leave the kernel.
-__device__ __forceinline__ bool grid_barrier(const GridSync &gs) {
+__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier for co-resident (cooperatively launched) blocks on a
+// monotone arrival counter: barrier number k completes when the counter
+// reaches k * gridDim.x, so nothing is reset and a block never waits on a
+// generation flag.  `epoch` is the caller's barrier count (identical in every
+// block).  The release add publishes this block's writes (bar.sync orders the
+// other threads' writes before it); the acquire load orders everything after.
+// Returns false when the wait gave up; the caller must then leave the kernel.
+__device__ __forceinline__ bool grid_barrier(const GridSync &gs, unsigned long long &epoch) {
     __shared__ int s_ok;
+    epoch += gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int *vgen = gs.gen;
-        const unsigned int my_gen = *vgen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(gs.count, 1u);
+        red_release_add_u64(gs.count, 1ull);
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(gs.count, 0u);
-            __threadfence();
-            atomicAdd(gs.gen, 1u);
-        } else {
-            uint32_t spins = 0;
-            while (*vgen == my_gen) {
-                if (++spins > kBarrierSpinLimit) {
-                    atomicCAS(gs.error, 0, kStatusTimeout);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(128);
+        uint32_t spins = 0;
+        while (ld_acquire_u64(gs.count) < epoch) {
+            if (++spins > kBarrierSpinLimit) {
+                atomicCAS(gs.error, 0, kStatusTimeout);
+                ok = 0;
+                break;
             }
+            if (spins > kTightSpins) __nanosleep(64);
         }
-        __threadfence();
-        if (*((volatile int *)gs.error) != 0) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
@@ -127,19 +131,29 @@ __device__ __forceinline__ void publish_partials(double (&v)[NV], double *partia
     }
 }
 
-// Grid reduction, step 2 (after a barrier): every block sums all partials in
-// the same fixed order, so every block holds bit-identical results.
+// Grid reduction, step 2 (after a barrier): warp 0 of every block sums all
+// partials in the same fixed order (lane-strided, then a fixed shuffle tree)
+// and broadcasts through shared memory, so every block holds bit-identical
+// results.
 template <int NV>
 __device__ __forceinline__ void gather_partials(const double *partials, double (&out)[NV],
                                                 double *smem) {
     const int G = gridDim.x;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double s = 0.0;
-        for (int j = threadIdx.x; j < G; j += blockDim.x) s += __ldcg(&partials[k * G + j]);
-        out[k] = s;
+        for (int k = 0; k < NV; ++k) {
+            double s = 0.0;
+            for (int j = lane; j < G; j += 32) s += __ldcg(&partials[k * G + j]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) smem[k] = s;
+        }
     }
-    block_sum<NV>(out, smem);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = smem[k];
+    __syncthreads();
 }
 
 template <int NV>
@@ -155,13 +169,21 @@ template <int NV>
 __device__ __forceinline__ void gather_max(const double *partials, double (&out)[NV],
                                            double *smem) {
     const int G = gridDim.x;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double s = 0.0;
-        for (int j = threadIdx.x; j < G; j += blockDim.x) s = fmax(s, __ldcg(&partials[k * G + j]));
-        out[k] = s;
+        for (int k = 0; k < NV; ++k) {
+            double s = 0.0;
+            for (int j = lane; j < G; j += 32) s = fmax(s, __ldcg(&partials[k * G + j]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+            if (lane == 0) smem[k] = s;
+        }
     }
-    block_max<NV>(out, smem);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = smem[k];
+    __syncthreads();
 }
 
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }

@@ -8,7 +8,7 @@
 // passes device-resident inputs and the output vector; every other byte the
 // solve needs comes from one file-scope __device__ array of fixed size.
 //
-// Limits: at most kMaxRows rows and kMaxNnz nonzeros (about 5.4 MB of device
+// Limits: at most kMaxRows rows and kMaxNnz nonzeros (about 6.2 MB of device
 // memory, held by every GPU that loads this library until the process exits).
 // Set-up: the first call on a device looks up that device's address of the
 // array (cudaGetSymbolAddress, with the device current); make that first call
@@ -35,8 +35,8 @@ constexpr int kMaxDevices = 64;
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Scratch layout (byte offsets), each region 256-byte aligned.
-constexpr size_t kOffVec = 0;                                               // 12 x rows x 8
-constexpr size_t kOffR64 = kOffVec + align256(12 * kMaxRows * 8);
+constexpr size_t kOffVec = 0;                                               // 15 x rows x 8
+constexpr size_t kOffR64 = kOffVec + align256(15 * kMaxRows * 8);
 constexpr size_t kOffDx = kOffR64 + align256(kMaxRows * 8);
 constexpr size_t kOffPartials = kOffDx + align256(kMaxRows * 8);            // 8 x grid doubles
 constexpr size_t kOffPartner = kOffPartials + align256(8 * kMaxGrid * 8);
@@ -44,7 +44,8 @@ constexpr size_t kOffDiag = kOffPartner + align256(kMaxRows * 4);
 constexpr size_t kOffOff = kOffDiag + align256(kMaxRows * 4);
 constexpr size_t kOffCand = kOffOff + align256(kMaxRows * 4);
 constexpr size_t kOffChoice = kOffCand + align256(kMaxRows * 4);
-constexpr size_t kOffVals32 = kOffChoice + align256(kMaxRows * 4);
+constexpr size_t kOffFlag = kOffChoice + align256(kMaxRows * 4);
+constexpr size_t kOffVals32 = kOffFlag + align256(kMaxRows);
 constexpr size_t kOffSync = kOffVals32 + align256(kMaxNnz * 4);            // 4 words + check flag
 constexpr size_t kOffInfo = kOffSync + 256;
 constexpr size_t kScratchBytes = kOffInfo + align256(sizeof(DeviceInfo));
@@ -143,6 +144,16 @@ __global__ void pc_pair_kernel(int n, const uint32_t *rp, const uint32_t *col, c
     }
 }
 
+// rowflag[i] = 1 when row i or one of its columns is paired.
+__global__ void pc_flag_kernel(int n, const uint32_t *rp, const uint32_t *col, const int32_t *partner,
+                               uint8_t *flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        bool f = partner[i] >= 0;
+        for (uint32_t k = rp[i]; k < rp[i + 1] && !f; ++k) f = partner[col[k]] >= 0;
+        flag[i] = f ? 1 : 0;
+    }
+}
+
 int small_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1024)); }
 
 }  // namespace
@@ -177,6 +188,7 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
     uint32_t *cand = (uint32_t *)(base + kOffCand);
     int32_t *choice = (int32_t *)(base + kOffChoice);
     float *vals32 = (float *)(base + kOffVals32);
+    uint8_t *rowflag = (uint8_t *)(base + kOffFlag);
 
     // validate the caller's CSR before any kernel indexes with it
     unsigned int bad = 0;
@@ -195,7 +207,8 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
         if (params->precond == OHM_PRECOND_AUTO) {
             pc_choose_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, d_values, diag, cand, choice);
             pc_pair_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, cand, choice, partner, off);
-            launches += 2;
+            pc_flag_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, partner, rowflag);
+            launches += 3;
         }
     } else {
         CUDA_TRY(cudaMemsetAsync(partner, 0xFF, n * sizeof(int32_t), s));   // -1: unpaired
@@ -221,10 +234,12 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
     a.partner = partner;
     a.diag_slot = diag;
     a.off_slot = off;
+    a.rowflag = params->precond == OHM_PRECOND_AUTO ? rowflag : nullptr;
     double *vec = (double *)(base + kOffVec);
-    void **slots[] = {&a.r, &a.rhat, &a.p0, &a.p1, &a.v, &a.s, &a.t, &a.phat, &a.shat, &a.d,
-                      &a.pc_self, &a.pc_part};
-    for (int k = 0; k < 12; ++k) *slots[k] = (void *)(vec + (size_t)k * n);
+    a.rec0 = (void *)vec;
+    a.rec1 = (void *)(vec + 4 * (size_t)n);
+    void **slots[] = {&a.rhat, &a.s, &a.t, &a.phat, &a.shat, &a.d, &a.pc_part};
+    for (int k = 0; k < 7; ++k) *slots[k] = (void *)(vec + (8 + (size_t)k) * n);
     a.r64 = (double *)(base + kOffR64);
     a.dx = (double *)(base + kOffDx);
     a.partials = (double *)(base + kOffPartials);

@@ -56,6 +56,12 @@ enum SolveStatus : int {
 
 enum PrecondKind : int { kPcAuto = 0, kPcJacobi = 1, kPcIsai = 2, kPcNone = 3 };
 
+// Threads per block of the persistent solver (one block per SM).
+#ifndef OHM_SOLVER_BLOCK
+#define OHM_SOLVER_BLOCK 1024
+#endif
+constexpr int kSolverBlock = OHM_SOLVER_BLOCK;
+
 // Breakdown test: |(a, b)| < kBreakdownRel * ||a|| ||b||.  The reference's
 // absolute 1e-30 (bicgstab.rs:107, :125) depends on the units of the
 // residual; a relative test only fires on (near-)exact orthogonality.
@@ -93,10 +99,14 @@ struct KernelArgs {
     const int32_t *partner;     // -1: unpaired
     const uint32_t *diag_slot;  // CSR slot of (i,i), kSentinel if absent
     const uint32_t *off_slot;   // CSR slot of (i, partner(i))
-    void *pc_self, *pc_part;    // Krylov-precision arrays
+    const uint8_t *rowflag;     // 1: row i or one of its columns is paired
+    void *pc_part;              // Krylov-precision coefficient on the partner
 
-    // Krylov vectors (8-byte slots; used as float or double); p is double-buffered
-    void *r, *rhat, *p0, *p1, *v, *s, *t, *phat, *shat, *d;
+    // Krylov state.  rec0/rec1: per-row records {p, v, r, c} (c = the
+    // preconditioner's self coefficient), double-buffered; the SpMV of each
+    // phase gathers one record (one 32-byte sector in FP64) per nonzero and
+    // forms M^-1 p or M^-1 s on the fly.  Other vectors: own rows only.
+    void *rec0, *rec1, *rhat, *s, *t, *phat, *shat, *d;
 
     // nonlinear devices and the stamp map
     int nd, nq, nm;
@@ -119,7 +129,12 @@ struct KernelArgs {
     int max_krylov;
     double krylov_tol;          // ||r|| < krylov_tol * ||b||  (bicgstab.rs:98)
     double inner_rtol;          // ... or < inner_rtol * ||r0|| (inexact inner solve)
+    int forcing;                // 1: Eisenstat-Walker inner tolerance, floor inner_rtol
+    double eta_max;             // Eisenstat-Walker upper bound
+    int fp32_max_iterations;    // mixed: iteration cap of an FP32 attempt before FP64
     int max_restarts;           // restarts with r_hat = r after a breakdown
+    double *trace;              // optional per-outer-iteration record (kTraceCols doubles)
+    int trace_cap;
     int require_true_residual;  // linear: fail unless the FP64 residual meets the tolerance
 
     double *partials;           // >= 8 * gridDim.x doubles (two alternating regions)
@@ -127,12 +142,18 @@ struct KernelArgs {
     DeviceInfo *info;
 };
 
-// Per-block view of the launch: row range and the reduction buffers.
+// Columns of the per-outer-iteration trace: FP32 Krylov iterations, FP64
+// Krylov iterations, ||b - J x|| (FP64) before the solve, inner tolerance
+// used, max|x - x_old| after limiting, restarts.
+constexpr int kTraceCols = 6;
+
+// Per-block view of the launch: row range, barrier epoch, reduction buffers.
 struct Grid {
     int G, bid, r0, r1, gtid, gstride;
     double *smem;
     double *partials;
     int red;
+    unsigned long long epoch;
     GridSync gs;
 
     // Consecutive grid reductions alternate between two partial regions: a
@@ -148,35 +169,72 @@ struct Grid {
 template <typename T>
 __device__ __forceinline__ T cvt(double x) { return (T)x; }
 
-// y_i = sum_j A_ij x_j for the rows of this block; `f(row, y_i)` runs on the
-// first lane of each row group.  All lanes of a warp run the same number of
-// tiles, so the group shuffles are safe.
-template <int LPR, typename TA, typename TX, typename F>
+// y_i = sum_j A_ij x(j) for the rows of this block, where x(j, slow) is a
+// gather functor; `f(row, y_i)` runs on the first lane of each row group.
+// Each group keeps kRowsInFlight rows in flight (their row pointers, nonzeros
+// and gathers are issued together), so the dependent L2 round trips of one row
+// overlap those of the others.  All lanes of a warp run the same number of
+// tiles and inner steps, so the group shuffles are safe.  `slow` is the row's
+// flag from `rowflag` (false when null).
+constexpr int kRowsInFlight = 4;
+
+template <int LPR, typename Acc, typename TA, typename X, typename F>
 __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
                                           const uint32_t *__restrict__ col,
-                                          const TA *__restrict__ val, const TX *__restrict__ x,
-                                          int r0, int r1, F f) {
-    using Acc = typename std::conditional<(sizeof(TA) > 4 || sizeof(TX) > 4), double, float>::type;
+                                          const TA *__restrict__ val, const uint8_t *rowflag,
+                                          int r0, int r1, X x, F f) {
+    constexpr int U = kRowsInFlight;
     const int lane = threadIdx.x % LPR;
     const int group = threadIdx.x / LPR;
     const int ngroups = blockDim.x / LPR;
-    for (int tile = r0; tile < r1; tile += ngroups) {
-        const int row = tile + group;
-        Acc acc = 0;
-        if (row < r1) {
-            const uint32_t e = rp[row + 1];
-            for (uint32_t k = rp[row] + lane; k < e; k += LPR)
-                acc += (Acc)val[k] * (Acc)x[col[k]];
+    for (int tile = r0; tile < r1; tile += ngroups * U) {
+        int row[U];
+        uint32_t beg[U], end[U];
+        bool slow[U];
+        Acc acc[U];
+        uint32_t len = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            row[u] = tile + group + u * ngroups;
+            const bool ok = row[u] < r1;
+            beg[u] = ok ? rp[row[u]] : 0u;
+            end[u] = ok ? rp[row[u] + 1] : 0u;
+            slow[u] = ok && rowflag != nullptr && rowflag[row[u]] != 0;
+            acc[u] = Acc(0);
         }
 #pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LPR);
-        if (lane == 0 && row < r1) f(row, (double)acc);
+        for (int u = 0; u < U; ++u) len = max(len, end[u] - beg[u]);
+        // the longest row of the group decides the step count; shuffles below
+        // need every lane of the warp, so take the warp-wide maximum
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+        for (uint32_t off = lane; off < len; off += LPR) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t k = beg[u] + off;
+                if (k < end[u]) acc[u] += (Acc)val[k] * (Acc)x((int)col[k], slow[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o, LPR);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (lane == 0 && row[u] < r1) f(row[u], (double)acc[u]);
     }
 }
 
-#define OHM_SYNC_OR(ret)                          \
-    do {                                          \
-        if (!grid_barrier(g.gs)) return ret;      \
+// Per-row Krylov record: p, v, r and the preconditioner's self coefficient.
+template <typename T>
+struct alignas(4 * sizeof(T)) KRec {
+    T p, v, r, c;
+};
+
+#define OHM_SYNC_OR(ret)                               \
+    do {                                               \
+        if (!grid_barrier(g.gs, g.epoch)) return ret;  \
     } while (0)
 
 struct KrylovOut {
@@ -184,17 +242,25 @@ struct KrylovOut {
     int restarts;
 };
 
-// Right-preconditioned BiCGSTAB on J d = r64 in precision T, d0 = 0.
-// Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On success the
-// correction is left in a.dx (FP64) for the rows of this block.
+// Right-preconditioned BiCGSTAB on J d = r64 in precision T, d0 = 0, with
+// the reference's operation order (bicgstab.rs:104-183) and three grid
+// synchronisations per iteration:
+//   AB: p = (p - w v) b + r and v = A M^-1 p  (M^-1 p formed on the fly per
+//       gathered record), reduce (r_hat, v), (v, v)
+//   CD: s = r - a v and t = A M^-1 s (on the fly), reduce (s, s), (t, s), (t, t)
+//   E : d += a phat + w shat; r = s - w t, reduce (r_hat, r), (r, r)
+// The early exit on ||s|| (bicgstab.rs:134-139) is taken after CD; t is then
+// simply unused.  Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On
+// success the correction is left in a.dx (FP64) for the rows of this block.
 template <typename T, int LPR>
 __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
-                                   bool accept_partial, KrylovOut &out) {
+                                      int max_it, bool accept_partial, KrylovOut &out) {
+    using Acc = T;   // FP32 SpMV accumulates in FP32, FP64 in FP64; dots always in FP64
     const int r0 = g.r0, r1 = g.r1;
-    T *r = (T *)a.r, *rhat = (T *)a.rhat, *v = (T *)a.v, *s = (T *)a.s, *t = (T *)a.t;
-    T *phat = (T *)a.phat, *shat = (T *)a.shat, *d = (T *)a.d;
-    T *pc_self = (T *)a.pc_self, *pc_part = (T *)a.pc_part;
-    T *pin = (T *)a.p0, *pout = (T *)a.p1;
+    KRec<T> *cur = (KRec<T> *)a.rec0, *nxt = (KRec<T> *)a.rec1;
+    T *rhat = (T *)a.rhat, *s = (T *)a.s, *t = (T *)a.t;
+    T *phat = (T *)a.phat, *shat = (T *)a.shat, *d = (T *)a.d, *pc_part = (T *)a.pc_part;
+    const int32_t *partner = a.partner;
     const T *A;
     if constexpr (sizeof(T) == 4) A = (const T *)a.vals32; else A = (const T *)a.vals64;
     out.iterations = 0;
@@ -204,13 +270,11 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
     double acc0[1] = {0.0};
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         const T rt = cvt<T>(a.r64[i]);
-        r[i] = rt; rhat[i] = rt; pin[i] = T(0); v[i] = T(0); d[i] = T(0);
-        acc0[0] += (double)rt * (double)rt;
         double cs = 0.0, cp = 0.0;
         if (a.precond != kPcNone) {
             const uint32_t ds = a.diag_slot[i];
             const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
-            const int pi = a.partner[i];
+            const int pi = partner[i];
             if (a.precond == kPcAuto && pi >= 0) {
                 const double akk = a.diag_slot[pi] == kSentinel ? 0.0 : a.vals64[a.diag_slot[pi]];
                 const double aik = a.vals64[a.off_slot[i]];
@@ -225,8 +289,13 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
         } else {
             cs = 1.0;
         }
-        pc_self[i] = cvt<T>(cs);
+        KRec<T> q;
+        q.p = T(0); q.v = T(0); q.r = rt; q.c = cvt<T>(cs);
+        cur[i] = q;
         pc_part[i] = cvt<T>(cp);
+        rhat[i] = rt;
+        d[i] = T(0);
+        acc0[0] += (double)rt * (double)rt;
     }
     {
         double *pr = g.part();
@@ -242,23 +311,33 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
     double rho = 1.0, alpha = 1.0, omega = 1.0;
     int code = kKrylovRunning;
     int it = 0;
+
+    // restart: r_hat = r, p = v = 0.  The shadow residual r_hat = b
+    // (bicgstab.rs:87) can be orthogonal to later residuals when b lives on a
+    // few source rows.
+#define OHM_RESTART()                                                          \
+    do {                                                                       \
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {              \
+            KRec<T> q = cur[i];                                                \
+            q.p = T(0); q.v = T(0);                                            \
+            cur[i] = q;                                                        \
+            rhat[i] = q.r;                                                     \
+        }                                                                      \
+        OHM_SYNC_OR(kKrylovAbort);                                             \
+        rho = 1.0; alpha = 1.0; omega = 1.0;                                   \
+        rho_new = rr_cur; rhat2 = rr_cur;                                      \
+        ++out.restarts;                                                        \
+    } while (0)
+
     if (!isfinite(r0norm)) {
         code = kKrylovNan;
     } else if (r0norm < abs_tol || r0norm == 0.0) {
         code = kKrylovConverged;
     } else {
-        for (; it < a.max_krylov; ++it) {
+        for (; it < max_it; ++it) {
             if (!(fabs(rho_new) >= kBreakdownRel * sqrt(rhat2 * rr_cur))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
-                    // restart: the shadow residual r_hat = b (bicgstab.rs:87) can be
-                    // orthogonal to later residuals when b lives on a few source rows
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                        rhat[i] = r[i]; pin[i] = T(0); v[i] = T(0);
-                    }
-                    OHM_SYNC_OR(kKrylovAbort);
-                    rho = 1.0; alpha = 1.0; omega = 1.0;
-                    rho_new = rr_cur; rhat2 = rr_cur;
-                    ++out.restarts;
+                    OHM_RESTART();
                 } else {
                     code = kKrylovBreakRho;
                     break;
@@ -266,27 +345,32 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
             }
             const double beta = (rho_new / rho) * (alpha / omega);
             rho = rho_new;
-            // p = (p - omega v) * beta + r ; phat = M^-1 p
-            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                const T pt = cvt<T>(((double)pin[i] + (-omega) * (double)v[i]) * beta + (double)r[i]);
-                pout[i] = pt;
-                double z = (double)pc_self[i] * (double)pt;
-                const int pi = a.partner[i];
-                if (pi >= 0) {
-                    const T pk = cvt<T>(((double)pin[pi] + (-omega) * (double)v[pi]) * beta + (double)r[pi]);
-                    z += (double)pc_part[i] * (double)pk;
+            const double om = omega;
+            // ---------------- AB: p update and v = A M^-1 p ----------------
+            auto pnew = [&](const KRec<T> &q) -> T {
+                return cvt<T>(((double)q.p + (-om) * (double)q.v) * beta + (double)q.r);
+            };
+            auto phat_at = [&](int j, bool slow) -> T {
+                const KRec<T> q = cur[j];
+                double z = (double)q.c * (double)pnew(q);
+                if (slow) {
+                    const int pj = partner[j];
+                    if (pj >= 0) z += (double)pc_part[j] * (double)pnew(cur[pj]);
                 }
-                phat[i] = cvt<T>(z);
-            }
-            { T *tmp = pin; pin = pout; pout = tmp; }
-            OHM_SYNC_OR(kKrylovAbort);
-            // v = A phat ; (r_hat, v), (v, v)
+                return cvt<T>(z);
+            };
             double acc1[2] = {0.0, 0.0};
-            spmv_rows<LPR>(a.row_ptr, a.col, A, phat, r0, r1, [&](int i, double y) {
-                const T yt = cvt<T>(y);
-                v[i] = yt;
-                acc1[0] += (double)rhat[i] * (double)yt;
-                acc1[1] += (double)yt * (double)yt;
+            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, phat_at, [&](int i, double y) {
+                const KRec<T> q = cur[i];
+                KRec<T> o;
+                o.p = pnew(q);
+                o.v = cvt<T>(y);
+                o.r = q.r;
+                o.c = q.c;
+                nxt[i] = o;
+                phat[i] = phat_at(i, true);
+                acc1[0] += (double)rhat[i] * (double)o.v;
+                acc1[1] += (double)o.v * (double)o.v;
             });
             {
                 double *pr = g.part();
@@ -296,68 +380,59 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
             }
             if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                        rhat[i] = r[i]; pin[i] = T(0); v[i] = T(0);
-                    }
-                    OHM_SYNC_OR(kKrylovAbort);
-                    rho = 1.0; alpha = 1.0; omega = 1.0;
-                    rho_new = rr_cur; rhat2 = rr_cur;
-                    ++out.restarts;
+                    OHM_RESTART();        // cur still holds r; restart from it
                     continue;
                 }
                 code = kKrylovBreakRv;
                 break;
             }
             alpha = rho / acc1[0];
-            // s = r - alpha v ; shat = M^-1 s ; ||s||^2
-            double acc2[1] = {0.0};
-            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                const T st = cvt<T>((double)r[i] + (-alpha) * (double)v[i]);
-                s[i] = st;
-                acc2[0] += (double)st * (double)st;
-                double z = (double)pc_self[i] * (double)st;
-                const int pi = a.partner[i];
-                if (pi >= 0) {
-                    const T sk = cvt<T>((double)r[pi] + (-alpha) * (double)v[pi]);
-                    z += (double)pc_part[i] * (double)sk;
+            const double al = alpha;
+            // ---------------- CD: s = r - a v and t = A M^-1 s ----------------
+            auto s_of = [&](const KRec<T> &q) -> T {
+                return cvt<T>((double)q.r + (-al) * (double)q.v);
+            };
+            auto shat_at = [&](int j, bool slow) -> T {
+                const KRec<T> q = nxt[j];
+                double z = (double)q.c * (double)s_of(q);
+                if (slow) {
+                    const int pj = partner[j];
+                    if (pj >= 0) z += (double)pc_part[j] * (double)s_of(nxt[pj]);
                 }
-                shat[i] = cvt<T>(z);
-            }
+                return cvt<T>(z);
+            };
+            double acc3[3] = {0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t)
+            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, shat_at, [&](int i, double y) {
+                const T si = s_of(nxt[i]);
+                const T ti = cvt<T>(y);
+                s[i] = si;
+                t[i] = ti;
+                shat[i] = shat_at(i, true);
+                acc3[0] += (double)si * (double)si;
+                acc3[1] += (double)ti * (double)si;
+                acc3[2] += (double)ti * (double)ti;
+            });
             {
                 double *pr = g.part();
-                publish_partials<1>(acc2, pr, g.smem);
+                publish_partials<3>(acc3, pr, g.smem);
                 OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<1>(pr, acc2, g.smem);
+                gather_partials<3>(pr, acc3, g.smem);
             }
-            if (sqrt(acc2[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
+            if (sqrt(acc3[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-                    d[i] = cvt<T>((double)d[i] + alpha * (double)phat[i]);
+                    d[i] = cvt<T>((double)d[i] + al * (double)phat[i]);
                 code = kKrylovConverged;
                 ++it;
                 break;
             }
-            // t = A shat ; (t, s), (t, t)
-            double acc3[2] = {0.0, 0.0};
-            spmv_rows<LPR>(a.row_ptr, a.col, A, shat, r0, r1, [&](int i, double y) {
-                const T yt = cvt<T>(y);
-                t[i] = yt;
-                acc3[0] += (double)yt * (double)s[i];
-                acc3[1] += (double)yt * (double)yt;
-            });
-            {
-                double *pr = g.part();
-                publish_partials<2>(acc3, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc3, g.smem);
-            }
-            if (!(acc3[1] > 0.0)) { code = kKrylovBreakTt; break; }
-            omega = acc3[0] / acc3[1];
-            // d += alpha phat ; d += omega shat ; r = s - omega t
+            if (!(acc3[2] > 0.0)) { code = kKrylovBreakTt; break; }
+            omega = acc3[1] / acc3[2];
+            // ---------------- E: d, r updates ----------------
             double acc4[2] = {0.0, 0.0};
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                d[i] = cvt<T>(((double)d[i] + alpha * (double)phat[i]) + omega * (double)shat[i]);
+                d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omega * (double)shat[i]);
                 const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
-                r[i] = rt;
+                nxt[i].r = rt;
                 acc4[0] += (double)rhat[i] * (double)rt;
                 acc4[1] += (double)rt * (double)rt;
             }
@@ -367,13 +442,14 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
                 OHM_SYNC_OR(kKrylovAbort);
                 gather_partials<2>(pr, acc4, g.smem);
             }
+            { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
             rho_new = acc4[0];
             rr_cur = acc4[1];
             const double rnorm = sqrt(acc4[1]);
             if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
             if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
             if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }
-            if (accept_partial && it + 1 == a.max_krylov && rnorm <= 0.5 * r0norm) {
+            if (accept_partial && it + 1 == max_it && rnorm <= 0.5 * r0norm) {
                 code = kKrylovConverged;          // inexact inner solve accepted
                 ++it;
                 break;
@@ -381,6 +457,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
         }
         if (code == kKrylovRunning) code = kKrylovMaxIter;
     }
+#undef OHM_RESTART
     out.iterations = it;
     if (code == kKrylovConverged)
         for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.dx[i] = (double)d[i];
@@ -388,7 +465,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
 }
 
 template <int LPR>
-__global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
+__global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
     __shared__ double smem[32 * 4];
     Grid g;
     g.G = gridDim.x;
@@ -400,6 +477,7 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
     g.smem = smem;
     g.partials = a.partials;
     g.red = 0;
+    g.epoch = 0;
     g.gs = a.gs;
     const int r0 = g.r0, r1 = g.r1, gtid = g.gtid, gstride = g.gstride;
 
@@ -407,6 +485,7 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
     int fallbacks = 0, restarts = 0;
     long long kiters = 0;
     double last_dmax = 0.0, bnorm_last = 0.0, final_res = -1.0;
+    double fnorm_prev = -1.0, eta_prev = a.eta_max;
 
     for (int outer = 0; outer < a.max_outer; ++outer) {
         // ---------------- device evaluation + stamping (Newton) ----------------
@@ -449,7 +528,10 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
 
         // -------------------------- FP64 residual r64 = b - A x -------------------------
         double acc[3] = {0.0, 0.0, 0.0};   // ||b||^2, ||r||^2, #non-finite
-        spmv_rows<LPR>(a.row_ptr, a.col, a.vals64, a.x, r0, r1, [&](int i, double ax) {
+        const double *xv = a.x;
+        auto x_at = [&](int j, bool) -> double { return xv[j]; };
+        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at,
+                               [&](int i, double ax) {
             const double bi = a.b[i];
             const double ri = bi - ax;
             a.r64[i] = ri;
@@ -483,24 +565,46 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
 
         // -------------------------------- BiCGSTAB ---------------------------------
         const double floor_tol = a.krylov_tol * bnorm;
+        // Inner tolerance: constant, or Eisenstat-Walker choice 2 (gamma 0.9,
+        // exponent 2, safeguarded) on the Newton residual ||b - J x||.
+        double eta = a.inner_rtol;
+        if (a.newton && a.forcing == 1) {
+            if (fnorm_prev > 0.0) {
+                const double ratio = rnorm64 / fnorm_prev;
+                eta = 0.9 * ratio * ratio;
+                const double guard = 0.9 * eta_prev * eta_prev;
+                if (guard > 0.1) eta = fmax(eta, guard);
+            } else {
+                eta = a.eta_max;
+            }
+            eta = fmin(fmax(eta, a.inner_rtol), a.eta_max);
+            eta_prev = eta;
+            fnorm_prev = rnorm64;
+        }
         KrylovOut ko{0, 0};
+        int it32 = 0, it64 = 0;
         if (a.mixed) {
-            kcode = krylov<float, LPR>(a, g, floor_tol, a.inner_rtol, true, ko);
+            kcode = krylov<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, a.max_krylov), true, ko);
             if (kcode == kKrylovAbort) return;
-            kiters += ko.iterations;
+            it32 = ko.iterations;
             restarts += ko.restarts;
             if (kcode != kKrylovConverged) {
                 ++fallbacks;           // FP32 failed or stalled: redo this solve in FP64
-                kcode = krylov<double, LPR>(a, g, floor_tol, a.inner_rtol, false, ko);
+                kcode = krylov<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
                 if (kcode == kKrylovAbort) return;
-                kiters += ko.iterations;
+                it64 = ko.iterations;
                 restarts += ko.restarts;
             }
         } else {
-            kcode = krylov<double, LPR>(a, g, floor_tol, a.inner_rtol, false, ko);
+            kcode = krylov<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
             if (kcode == kKrylovAbort) return;
-            kiters += ko.iterations;
+            it64 = ko.iterations;
             restarts += ko.restarts;
+        }
+        kiters += it32 + it64;
+        if (a.trace && outer < a.trace_cap && g.bid == 0 && threadIdx.x == 0) {
+            double *tr = a.trace + (size_t)outer * kTraceCols;
+            tr[0] = it32; tr[1] = it64; tr[2] = rnorm64; tr[3] = eta; tr[4] = -1.0; tr[5] = ko.restarts;
         }
         if (kcode != kKrylovConverged) {
             status = kErrSolve;
@@ -549,6 +653,8 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
             gather_max<3>(pr, mx, g.smem);
             last_dmax = mx[0];
             outer_done = outer + 1;
+            if (a.trace && outer < a.trace_cap && g.bid == 0 && threadIdx.x == 0)
+                a.trace[(size_t)outer * kTraceCols + 4] = mx[0];
             if (mx[2] > 0.0) { status = kErrNewtonNumerical; err_iter = outer; break; }
             if (mx[0] < a.abs_tol + a.rel_tol * mx[1]) { status = kOk; break; }
             if (outer + 1 == a.max_outer) status = kErrNewtonNotConverged;
@@ -558,7 +664,10 @@ __global__ void __launch_bounds__(512, 1) persistent_solver(KernelArgs a) {
     // final FP64 residual of a linear solve (reported; the refinement test in mixed mode)
     if (!a.newton && status == kOk && final_res < 0.0) {
         double acc[1] = {0.0};
-        spmv_rows<LPR>(a.row_ptr, a.col, a.vals64, a.x, r0, r1, [&](int i, double ax) {
+        const double *xv = a.x;
+        auto x_at = [&](int j, bool) -> double { return xv[j]; };
+        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at,
+                               [&](int i, double ax) {
             const double ri = a.b[i] - ax;
             acc[0] += ri * ri;
         });

@@ -86,6 +86,7 @@ class BiCgStabParams:
     inner_rtol: float = 0.0
     max_refinements: int = 1
     max_restarts: int = 50
+    fp32_max_iterations: int = 600
 
     def to_c(self) -> _lib.KrylovParams:
         p = _lib.KrylovParams()
@@ -97,6 +98,7 @@ class BiCgStabParams:
         p.inner_rtol = float(self.inner_rtol)
         p.max_refinements = int(self.max_refinements)
         p.max_restarts = int(self.max_restarts)
+        p.fp32_max_iterations = int(self.fp32_max_iterations)
         return p
 
 
@@ -112,6 +114,9 @@ class NewtonParams:
     precision: int = _lib.PREC_FP64
     precond: int = _lib.PRECOND_AUTO
     inner_rtol: float = 0.0
+    forcing: int = 0              # 0 constant inner_rtol, 1 Eisenstat-Walker
+    eta_max: float = 0.5
+    fp32_max_iterations: int = 600
 
     def to_c(self):
         p = _lib.NewtonParamsC()
@@ -120,7 +125,10 @@ class NewtonParams:
         p.abs_tol = float(self.abs_tol)
         p.rel_tol = float(self.rel_tol)
         p.krylov = BiCgStabParams(self.bicgstab_max_iterations, self.bicgstab_tolerance,
-                                  self.precision, self.precond, self.inner_rtol).to_c()
+                                  self.precision, self.precond, self.inner_rtol,
+                                  fp32_max_iterations=self.fp32_max_iterations).to_c()
+        p.forcing = int(self.forcing)
+        p.eta_max = float(self.eta_max)
         keep = None
         if self.initial_guess is not None:
             keep = np.ascontiguousarray(self.initial_guess, dtype=np.float64)
@@ -294,6 +302,17 @@ class NewtonPlan:
         if st != _lib.OK:
             _raise(st, info)
         return self.last_info
+
+    def trace(self):
+        """Per-Newton-iteration record of the last newton_device call (rows x 6)."""
+        out = np.zeros((256, 6))
+        rows = C.c_int32()
+        st = self.ctx.lib.ohm_plan_trace(self._h, dptr(out), 256, C.byref(rows))
+        if st:
+            _raise(st)
+        t = out[: rows.value]
+        keep = ~np.all(np.isnan(t), axis=1)
+        return t[keep]
 
     def assemble(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
