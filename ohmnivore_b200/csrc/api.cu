@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "isai_host.h"
 
 using namespace ohm;
 
@@ -409,6 +410,74 @@ struct Workspace {
     }
 };
 
+// Device copy of the ISAI(1) structure (isai_host.h) plus its value arrays.
+struct IsaiDev {
+    bool ready = false;
+    uint32_t *aug_rp = nullptr, *aug_col = nullptr, *aug_diag = nullptr, *cp_ptr = nullptr, *cp_pair = nullptr;
+    int32_t *aug_map = nullptr;
+    double *f0 = nullptr, *f1 = nullptr, *ml_val = nullptr, *mu_val = nullptr;
+    uint32_t *ml_rp = nullptr, *ml_col = nullptr, *ml_cp = nullptr, *ml_row = nullptr, *ml_pos = nullptr;
+    uint32_t *mu_rp = nullptr, *mu_col = nullptr, *mu_cp = nullptr, *mu_row = nullptr, *mu_pos = nullptr;
+
+    void release() {
+        void *ptrs[] = {aug_rp, aug_col, aug_diag, cp_ptr, cp_pair, aug_map, f0, f1, ml_val, mu_val,
+                        ml_rp, ml_col, ml_cp, ml_row, ml_pos, mu_rp, mu_col, mu_cp, mu_row, mu_pos};
+        for (void *p : ptrs) cudaFree(p);
+        *this = IsaiDev{};
+    }
+    template <typename T>
+    static cudaError_t put(T **dst, const std::vector<T> &v, cudaStream_t s) {
+        cudaError_t e = dalloc(dst, v.size());
+        if (e == cudaSuccess && !v.empty()) e = cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+        return e;
+    }
+    cudaError_t build(int64_t n, const uint32_t *rp, const uint32_t *col, cudaStream_t s) {
+        IsaiHost h;
+        h.build(n, rp, col);
+        cudaError_t e = put(&aug_rp, h.arp, s);
+        if (e == cudaSuccess) e = put(&aug_col, h.acol, s);
+        if (e == cudaSuccess) e = put(&aug_diag, h.adiag, s);
+        if (e == cudaSuccess) e = put(&aug_map, h.amap, s);
+        if (e == cudaSuccess) e = put(&cp_ptr, h.cptr, s);
+        if (e == cudaSuccess) e = put(&cp_pair, h.cpair, s);
+        if (e == cudaSuccess) e = put(&ml_rp, h.mlrp, s);
+        if (e == cudaSuccess) e = put(&ml_col, h.mlcol, s);
+        if (e == cudaSuccess) e = put(&ml_cp, h.mlcp, s);
+        if (e == cudaSuccess) e = put(&ml_row, h.mlrow, s);
+        if (e == cudaSuccess) e = put(&ml_pos, h.mlpos, s);
+        if (e == cudaSuccess) e = put(&mu_rp, h.murp, s);
+        if (e == cudaSuccess) e = put(&mu_col, h.mucol, s);
+        if (e == cudaSuccess) e = put(&mu_cp, h.mucp, s);
+        if (e == cudaSuccess) e = put(&mu_row, h.murow, s);
+        if (e == cudaSuccess) e = put(&mu_pos, h.mupos, s);
+        if (e == cudaSuccess) e = dalloc(&f0, h.nnz_aug);
+        if (e == cudaSuccess) e = dalloc(&f1, h.nnz_aug);
+        if (e == cudaSuccess) e = dalloc(&ml_val, h.mlcol.size());
+        if (e == cudaSuccess) e = dalloc(&mu_val, h.mucol.size());
+        // positions a column system leaves out stay zero
+        if (e == cudaSuccess) e = cudaMemsetAsync(ml_val, 0, std::max<size_t>(1, h.mlcol.size()) * sizeof(double), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(mu_val, 0, std::max<size_t>(1, h.mucol.size()) * sizeof(double), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // host vectors go out of scope
+        ready = e == cudaSuccess;
+        return e;
+    }
+    void bind(KernelArgs &a) const {
+        a.aug_rp = aug_rp; a.aug_col = aug_col; a.aug_diag = aug_diag; a.aug_map = aug_map;
+        a.cp_ptr = cp_ptr; a.cp_pair = cp_pair; a.isai_f0 = f0; a.isai_f1 = f1;
+        a.ml_rp = ml_rp; a.ml_col = ml_col; a.ml_cp = ml_cp; a.ml_row = ml_row; a.ml_pos = ml_pos; a.ml_val = ml_val;
+        a.mu_rp = mu_rp; a.mu_col = mu_col; a.mu_cp = mu_cp; a.mu_row = mu_row; a.mu_pos = mu_pos; a.mu_val = mu_val;
+    }
+};
+
+static int precond_kind(int p) {
+    switch (p) {
+        case OHM_PRECOND_NONE: return kPcNone;
+        case OHM_PRECOND_JACOBI: return kPcJacobi;
+        case OHM_PRECOND_ISAI1: return kPcIsai;
+        default: return kPcAuto;
+    }
+}
+
 ohm_status ohm_check_krylov(const ohm_krylov_params *p) {
     if (!p) return fail(OHM_ERR_INVALID_ARG, "params is null");
     if (p->max_iterations <= 0) return fail(OHM_ERR_SOLVE, "BiCGSTAB max_iterations must be > 0");
@@ -418,8 +487,6 @@ ohm_status ohm_check_krylov(const ohm_krylov_params *p) {
         return fail(OHM_ERR_INVALID_ARG, "unknown precision %d", p->precision);
     if (p->precond < 0 || p->precond > OHM_PRECOND_NONE)
         return fail(OHM_ERR_INVALID_ARG, "unknown preconditioner %d", p->precond);
-    if (p->precond == OHM_PRECOND_ISAI1)
-        return fail(OHM_ERR_INVALID_ARG, "ISAI(1) is not available in this build");
     return OHM_OK;
 }
 
@@ -449,6 +516,8 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     PcHost pc;
     build_precond(n, h_rp, h_col, h_val, {}, p->precond == OHM_PRECOND_AUTO, pc);
     e = ws.upload_pc(pc, c->stream);
+    IsaiDev isai;
+    if (e == cudaSuccess && p->precond == OHM_PRECOND_ISAI1) e = isai.build(n, h_rp, h_col, c->stream);
     if (e == cudaSuccess && mixed && nnz > 0) {
         f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, c->stream>>>(d_val, v32, nnz);
         e = cudaGetLastError();
@@ -459,8 +528,9 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     a.n = (int)n; a.nnz = (int)nnz;
     a.row_ptr = d_rp; a.col = d_col; a.vals64 = d_val; a.vals32 = v32;
     a.b = d_b; a.x = d_x;
-    a.precond = p->precond == OHM_PRECOND_NONE ? kPcNone : (p->precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
+    a.precond = precond_kind(p->precond);
     ws.bind(a);
+    if (isai.ready) isai.bind(a);
     a.newton = 0;
     a.mixed = mixed ? 1 : 0;
     a.max_outer = std::max(1, p->max_refinements);
@@ -475,6 +545,7 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     if (st == OHM_OK) st = finish_solver(c, info, launches);
     cudaStreamSynchronize(c->stream);
     ws.release();
+    isai.release();
     cudaFree(v32);
     return st;
 }
@@ -534,6 +605,7 @@ struct ohm_plan {
     unsigned long long *node_scale = nullptr;
     double *trace = nullptr;           // kTraceRows x kTraceCols
     Workspace ws;
+    IsaiDev isai;                      // built on the first ISAI(1) solve
     // host copies needed to rebuild the preconditioner when the base changes
     std::vector<uint32_t> h_rp, h_col;
     std::vector<char> touched;
@@ -552,6 +624,7 @@ static void plan_free(ohm_plan *p) {
     cudaFree(p->node_scale);
     cudaFree(p->trace);
     p->ws.release();
+    p->isai.release();
     delete p;
 }
 
@@ -723,8 +796,15 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.vals64 = p->vals64; a.vals32 = p->vals32;
     a.base_vals = p->base_vals; a.base_b = p->base_b; a.b = p->b;
     a.x = x_dev; a.x_prev = p->x_prev;
-    a.precond = kp.precond == OHM_PRECOND_NONE ? kPcNone : (kp.precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
+    a.precond = precond_kind(kp.precond);
     p->ws.bind(a);
+    if (kp.precond == OHM_PRECOND_ISAI1) {
+        if (!p->isai.ready) {
+            cudaError_t e = p->isai.build(p->n, p->h_rp.data(), p->h_col.data(), p->ctx->stream);
+            if (e != cudaSuccess) return fail(OHM_ERR_CUDA, "ISAI set-up: %s", cudaGetErrorString(e));
+        }
+        p->isai.bind(a);
+    }
     a.nd = (int)p->nd; a.nq = (int)p->nq; a.nm = (int)p->nm;
     a.diodes = p->diodes; a.bjts = p->bjts; a.mosfets = p->mosfets; a.bjt_vaf = p->vaf;
     a.mstamp = p->mstamp; a.rstamp = p->rstamp;

@@ -163,6 +163,9 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
                                              double *d_x, const ohm_krylov_params *params, ohm_solve_info *info) {
     ohm_status st = ohm_check_krylov(params);
     if (st != OHM_OK) return st;
+    if (params->precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "ohm_solve_real_noalloc: ISAI(1) needs allocated set-up; "
+                                             "use block Jacobi or ohm_solve_real");
     if (n < 0 || nnz < 0) return ohm_fail(OHM_ERR_INVALID_ARG, "negative size");
     if (n > kMaxRows || nnz > kMaxNnz)
         return ohm_fail(OHM_ERR_INVALID_ARG,

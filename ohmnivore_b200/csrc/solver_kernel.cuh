@@ -137,6 +137,17 @@ struct KernelArgs {
     int trace_cap;
     int require_true_residual;  // linear: fail unless the FP64 residual meets the tolerance
 
+    // ISAI(1): augmented pattern (A + diagonal), Chow-Patel product lists,
+    // factor values (double-buffered), M_L / M_U (CSR values + column lists)
+    const uint32_t *aug_rp, *aug_col, *aug_diag;
+    const int32_t *aug_map;
+    const uint32_t *cp_ptr, *cp_pair;
+    double *isai_f0, *isai_f1;
+    const uint32_t *ml_rp, *ml_col, *ml_cp, *ml_row, *ml_pos;
+    double *ml_val;
+    const uint32_t *mu_rp, *mu_col, *mu_cp, *mu_row, *mu_pos;
+    double *mu_val;
+
     double *partials;           // >= 8 * gridDim.x doubles (two alternating regions)
     GridSync gs;
     DeviceInfo *info;
@@ -464,6 +475,20 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
     return code;
 }
 
+}  // namespace ohm
+
+#include "isai.cuh"
+
+namespace ohm {
+
+// One Krylov solve of J d = r64 with the configured preconditioner.
+template <typename T, int LPR>
+__device__ __forceinline__ int krylov_any(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
+                                          int max_it, bool accept_partial, KrylovOut &out) {
+    if (a.precond == kPcIsai) return krylov_isai<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
+    return krylov<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
+}
+
 template <int LPR>
 __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
     __shared__ double smem[32 * 4];
@@ -563,6 +588,12 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
             break;
         }
 
+        // ISAI(1) factorisation of the current matrix (once per outer iteration
+        // of a Newton solve, once for a linear solve)
+        if (a.precond == kPcIsai && (a.newton || outer == 0)) {
+            if (!isai_setup(a, g)) return;
+        }
+
         // -------------------------------- BiCGSTAB ---------------------------------
         const double floor_tol = a.krylov_tol * bnorm;
         // Inner tolerance: constant, or Eisenstat-Walker choice 2 (gamma 0.9,
@@ -584,19 +615,19 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
         KrylovOut ko{0, 0};
         int it32 = 0, it64 = 0;
         if (a.mixed) {
-            kcode = krylov<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, a.max_krylov), true, ko);
+            kcode = krylov_any<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, a.max_krylov), true, ko);
             if (kcode == kKrylovAbort) return;
             it32 = ko.iterations;
             restarts += ko.restarts;
             if (kcode != kKrylovConverged) {
                 ++fallbacks;           // FP32 failed or stalled: redo this solve in FP64
-                kcode = krylov<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
+                kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
                 if (kcode == kKrylovAbort) return;
                 it64 = ko.iterations;
                 restarts += ko.restarts;
             }
         } else {
-            kcode = krylov<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
+            kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
             if (kcode == kKrylovAbort) return;
             it64 = ko.iterations;
             restarts += ko.restarts;

@@ -151,3 +151,38 @@ def test_backend_ops(ctx):
     ref = linear_ref.sparse_lu_solve(s.size, s.g.row_ptr, s.g.col, s.g.val, s.b_dc)
     assert _rel_err(bsol.download(), ref, slice(0, s.size)) < 1e-9
     assert info["kernel_launches"] >= 1
+
+
+# ---- ISAI(1) (src/solver/gpu.rs:139-168: the reference's choice for any zero diagonal) ----
+@pytest.mark.parametrize("case", [c for c in KA.REAL_SOLVES if c["name"] != "pivoting_3x3"],
+                         ids=lambda c: c["name"])
+def test_solve_real_isai_known_answers(ctx, case):
+    """ISAI(1) on the reference's known answers.  pivoting_3x3 has a zero
+    leading diagonal that needs row pivoting; ILU(0) in natural order cannot
+    factor it (MNA matrices order branch rows after node rows, so they can)."""
+    a = _mcsr(case)
+    x = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-14, precond=2)).solve_real(a, case["b"])
+    ax = linear_ref.spmv(a.nrows, a.row_ptr, a.col, a.val, x)
+    np.testing.assert_allclose(ax, case["b"], atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])
+def test_isai_ladder_and_mesh_vs_oracle(ctx, prec):
+    for sysm in (mna.compile_circuit(ck.resistor_ladder(2000, seed=0)),
+                 mna.compile_circuit(ck.diode_mesh(60, 60, seed=5, diode_frac=0.0))):
+        ref = linear_ref.sparse_lu_solve(sysm.size, sysm.g.row_ptr, sysm.g.col, sysm.g.val, sysm.b_dc)
+        p = S.BiCgStabParams(tolerance=1e-14, precond=2, precision=prec, max_refinements=20 if prec else 1)
+        solver = S.GpuSolver(ctx, p)
+        x = solver.solve_real(sysm.g, sysm.b_dc)
+        assert _rel_err(x, ref, slice(0, sysm.n_nodes)) < 1e-9
+
+
+def test_isai_fewer_iterations_than_jacobi(ctx):
+    """ISAI(1) from ILU(0) needs fewer BiCGSTAB iterations than (block) Jacobi on a mesh."""
+    sysm = mna.compile_circuit(ck.diode_mesh(80, 80, seed=6, diode_frac=0.0))
+    its = {}
+    for pc in (0, 2):
+        solver = S.GpuSolver(ctx, S.BiCgStabParams(tolerance=1e-10, precond=pc, max_iterations=50000))
+        solver.solve_real(sysm.g, sysm.b_dc)
+        its[pc] = solver.last_info["krylov_iterations"]
+    assert its[2] < its[0], its

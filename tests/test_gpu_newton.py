@@ -94,6 +94,20 @@ def test_newton_matches_oracle(ctx, make, prec):
     assert stats["kernel_launches"] == 1
 
 
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])
+def test_newton_isai_matches_oracle(ctx, prec):
+    """Newton with the ISAI(1) preconditioner refactored on the device every iteration."""
+    s = mna.compile_circuit(ck.diode_mesh(24, 24, seed=3))
+    ref, _ = newton_ref.newton(s)
+    p = _newton_params(prec)
+    p.precond = 2
+    stats = {}
+    x = S.newton_solve(ctx, s.g.val, s.g.col, s.g.row_ptr, s.b_dc, s.diode_descriptors,
+                       s.bjt_descriptors, s.mosfet_descriptors, s.size, s.g.nnz, p, stats)
+    assert _rel(x[: s.n_nodes], ref[: s.n_nodes]) < 1e-9
+    assert _rel(x[s.n_nodes:], ref[s.n_nodes:]) < 1e-9
+
+
 def test_newton_reference_defaults(ctx):
     """Reference NewtonParams defaults (abs_tol 1e-4, BiCGSTAB tol 1e-5 of
     ||b||) reach the operating point within the reference's own GPU-vs-CPU

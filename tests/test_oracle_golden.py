@@ -225,3 +225,86 @@ def test_pnjlim_reference_behaviour():
     assert abs(v - (0.6 + vt * (2 + math.log((1 + 4.4 / vt) - 2)))) < 1e-12
     v2 = float(devices_ref.pnjlim(5.0, -1.0, vt, vcrit))
     assert abs(v2 - vt * math.log(5.0 / vt)) < 1e-12
+
+
+# ---- ISAI known answers (src/solver/preconditioner.rs:509-820) ----
+from oracle import isai_ref  # noqa: E402
+
+_TRI3 = [(0, 0, 4.0), (0, 1, -1.0), (1, 0, -1.0), (1, 1, 4.0), (1, 2, -1.0), (2, 1, -1.0), (2, 2, 4.0)]
+
+
+def _ref_csr(n, trip):
+    a = RefCsr.from_triplets(n, n, trip)
+    return a.row_pointers, a.col_indices, a.values
+
+
+def test_isai_ilu0_reproduces_pa():
+    """preconditioner.rs:510-559: L*U == P*A, unit diagonal of L."""
+    rp, ci, v = _ref_csr(3, _TRI3)
+    L, U, perm = isai_ref.ilu0_ref(3, rp, ci, v)
+    A = RefCsr.from_triplets(3, 3, _TRI3).to_dense()
+    np.testing.assert_allclose(L @ U, A[perm], atol=1e-10)
+    np.testing.assert_allclose(np.diag(L), 1.0, atol=1e-14)
+
+
+def test_isai0_exact_for_diagonal():
+    """preconditioner.rs:561-606."""
+    rp, ci, v = _ref_csr(3, [(0, 0, 2.0), (1, 1, 4.0), (2, 2, 5.0)])
+    ML, MU, L, U, _ = isai_ref.compute_isai_ref(3, rp, ci, v, level=0)
+    np.testing.assert_allclose(ML @ L, np.eye(3), atol=1e-10)
+    np.testing.assert_allclose(MU @ U, np.eye(3), atol=1e-10)
+
+
+def test_isai1_tridiagonal_exact():
+    """preconditioner.rs:608-644: M_L * L = I with the L^2 pattern."""
+    rp, ci, v = _ref_csr(3, _TRI3)
+    ML, _, L, _, _ = isai_ref.compute_isai_ref(3, rp, ci, v, level=1)
+    np.testing.assert_allclose(ML @ L, np.eye(3), atol=1e-10)
+
+
+def test_isai_zero_diagonal_mna_finite():
+    """preconditioner.rs:706-736."""
+    g1, g2 = 0.001, 0.002
+    trip = [(0, 0, g1 + g2), (0, 1, -g2), (0, 2, 1.0), (1, 0, -g2), (1, 1, g2), (2, 0, 1.0)]
+    rp, ci, v = _ref_csr(3, trip)
+    ML, MU, _, _, _ = isai_ref.compute_isai_ref(3, rp, ci, v, level=0)
+    assert np.all(np.isfinite(ML)) and np.all(np.isfinite(MU))
+
+
+def test_isai_level1_better_than_level0():
+    """preconditioner.rs:738-791."""
+    trip = [(0, 0, 4.0), (0, 1, -1.0), (1, 0, -1.0), (1, 1, 4.0), (1, 2, -1.0), (2, 1, -1.0), (2, 2, 4.0),
+            (2, 3, -1.0), (3, 2, -1.0), (3, 3, 4.0)]
+    rp, ci, v = _ref_csr(4, trip)
+    ML0, _, L, _, _ = isai_ref.compute_isai_ref(4, rp, ci, v, level=0)
+    ML1, _, _, _, _ = isai_ref.compute_isai_ref(4, rp, ci, v, level=1)
+    e0 = np.sum((ML0 @ L - np.eye(4)) ** 2)
+    e1 = np.sum((ML1 @ L - np.eye(4)) ** 2)
+    assert e1 <= e0 + 1e-14
+
+
+def test_isai1_ill_conditioned_mna():
+    """preconditioner.rs:793-819: ISAI(1) closer to A^-1 than ISAI(0)."""
+    trip = [(0, 0, 1e-3 + 1e-12), (0, 1, -1e-3), (0, 3, 1.0), (1, 0, -1e-3), (1, 1, 1e-3 + 1e-12),
+            (2, 2, 1e-12), (2, 3, -1.0), (3, 0, 1.0), (3, 2, -1.0)]
+    rp, ci, v = _ref_csr(4, trip)
+    A = RefCsr.from_triplets(4, 4, trip).to_dense()
+    ML0, MU0, _, _, _ = isai_ref.compute_isai_ref(4, rp, ci, v, level=0)
+    ML1, MU1, _, _, _ = isai_ref.compute_isai_ref(4, rp, ci, v, level=1)
+    e0 = np.linalg.norm(MU0 @ ML0 @ A - np.eye(4))
+    e1 = np.linalg.norm(MU1 @ ML1 @ A - np.eye(4))
+    assert e1 < e0
+
+
+def test_ilu0_augmented_matches_lu_on_tridiagonal():
+    """The device factor (ILU(0) on A + diagonal) equals the exact LU when
+    there is no fill (tridiagonal) and gives a nonzero pivot on an MNA branch row."""
+    rp, ci, v = _ref_csr(3, _TRI3)
+    L, U = isai_ref.ilu0_augmented(3, rp, ci, v)
+    A = RefCsr.from_triplets(3, 3, _TRI3).to_dense()
+    np.testing.assert_allclose(L @ U, A, atol=1e-12)
+    g1, g2 = 0.001, 0.002
+    trip = [(0, 0, g1 + g2), (0, 1, -g2), (0, 2, 1.0), (1, 0, -g2), (1, 1, g2), (2, 0, 1.0)]
+    rp, ci, v = _ref_csr(3, trip)
+    L, U = isai_ref.ilu0_augmented(3, rp, ci, v)
+    assert abs(U[2, 2] - (-1.0 / (g1 + g2))) < 1e-9
