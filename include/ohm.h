@@ -179,6 +179,14 @@ ohm_status ohm_solve_real(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *
                           const uint32_t *col, const double *values, const double *b,
                           double *x, const ohm_krylov_params *params, ohm_solve_info *info);
 
+/* ISAI(1) preconditioner of A (host CSR) built on the device, applied to
+ * n_vectors host vectors r (n doubles each): z = M_U (M_L r).  M_L, M_U are
+ * the level-1 incomplete sparse approximate inverses of the ILU(0) factors
+ * (reference: compute_isai, src/solver/preconditioner.rs:239-277, and the
+ * apply of src/solver/gpu.rs:159-162).  For testing the set-up; one block. */
+ohm_status ohm_isai_apply(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *row_ptr, const uint32_t *col,
+                          const double *values, const double *r, double *z, int64_t n_vectors);
+
 /* Same on device-resident operands (no host copies). */
 ohm_status ohm_solve_real_device(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *b, ohm_buf *x,
                                  const ohm_krylov_params *params, ohm_solve_info *info);
@@ -240,6 +248,39 @@ ohm_status ohm_plan_download_system(ohm_plan *plan, double *values, double *rhs)
 ohm_status ohm_plan_assemble(ohm_plan *plan, const double *x_host, double *values_out, double *rhs_out);
 /* One limiting step: x_new_inout (host) is damped against x_old (host). */
 ohm_status ohm_plan_limit(ohm_plan *plan, const double *x_old_host, double *x_new_inout);
+
+/* ---------------------------------------------------------------- batches --
+ * Many independent nonlinear circuits solved by one launch (Monte Carlo
+ * corners, parameter sweeps).  No counterpart in the reference, which runs
+ * one circuit per call of newton_solve (src/solver/newton.rs:62-430); each
+ * instance here follows that same Newton loop.
+ *
+ * Packed layout, instance i owning:
+ *   rows       [row_off[i], row_off[i+1])            (its local size n_i)
+ *   nonzeros   [nnz_off[i], nnz_off[i+1])
+ *   row_ptrs   entries [row_off[i] + i, row_off[i+1] + i] (n_i + 1 local row
+ *              pointers starting at 0; local column indices)
+ *   devices    [diode_off[i], diode_off[i+1]) etc., with local node / value
+ *              indices in their descriptors.
+ * base_b and the solution vector are packed by rows.  Each instance is solved
+ * by one thread block with the block-Jacobi preconditioner (ISAI(1) is
+ * rejected), largest instances first. */
+typedef struct ohm_batch ohm_batch;
+ohm_status ohm_batch_create(ohm_ctx *ctx, int64_t n_instances, const int64_t *row_off, const int64_t *nnz_off,
+                            const uint32_t *row_ptrs, const uint32_t *col_indices,
+                            const double *base_g_values, const double *base_b,
+                            const int64_t *diode_off, const ohm_diode_desc *diodes,
+                            const int64_t *bjt_off, const ohm_bjt_desc *bjts, const double *bjt_vaf,
+                            const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets, ohm_batch **out);
+ohm_status ohm_batch_destroy(ohm_batch *batch);
+/* Newton on every instance.  x_inout_device: row_off[n] doubles.  `summary`
+ * gets totals (iterations = the largest Newton count, error_iteration = the
+ * first failed instance, -1 when all converged).  Returns the status
+ * of the first failed instance, if any. */
+ohm_status ohm_batch_newton_device(ohm_batch *batch, double *x_inout_device, const ohm_newton_params *params,
+                                   ohm_solve_info *summary);
+/* Per-instance results of the last ohm_batch_newton_device call. */
+ohm_status ohm_batch_instance_info(ohm_batch *batch, ohm_solve_info *infos, int64_t n_instances);
 
 #ifdef __cplusplus
 }

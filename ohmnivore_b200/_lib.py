@@ -89,6 +89,12 @@ SIGNATURES = {
     "ohm_plan_assemble": (C.c_int, [_vp, _dp, _dp, _dp]),
     "ohm_plan_limit": (C.c_int, [_vp, _dp, _dp]),
     "ohm_plan_trace": (C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int32)]),
+    "ohm_batch_create": (C.c_int, [_vp, _i64, _vp, _vp, _u32p, _u32p, _dp, _dp, _vp, _vp, _vp, _vp, _dp,
+                                   _vp, _vp, C.POINTER(_vp)]),
+    "ohm_batch_destroy": (C.c_int, [_vp]),
+    "ohm_isai_apply": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64]),
+    "ohm_batch_newton_device": (C.c_int, [_vp, _vp, C.POINTER(NewtonParamsC), C.POINTER(SolveInfo)]),
+    "ohm_batch_instance_info": (C.c_int, [_vp, C.POINTER(SolveInfo), _i64]),
 }
 
 _LIB = None

@@ -15,6 +15,7 @@
 
 #include "internal.cuh"
 #include "isai_host.h"
+#include "host_util.h"
 
 using namespace ohm;
 
@@ -127,121 +128,6 @@ extern "C" ohm_status ohm_ctx_synchronize(ohm_ctx *c) {
 }
 
 extern "C" void *ohm_ctx_stream(ohm_ctx *c) { return c ? (void *)c->stream : nullptr; }
-
-// ------------------------------------------------------------- validation --
-static ohm_status check_csr(int64_t n, int64_t nnz, const uint32_t *rp, const uint32_t *col) {
-    if (n < 0 || nnz < 0) return fail(OHM_ERR_INVALID_ARG, "negative size");
-    if (n > 0x7fffffffLL || nnz > 0xfffffffeLL) return fail(OHM_ERR_INVALID_ARG, "size exceeds u32 indexing");
-    if (!rp || (nnz > 0 && !col)) return fail(OHM_ERR_INVALID_ARG, "null CSR pointer");
-    if (rp[0] != 0) return fail(OHM_ERR_COMPILE, "row_ptr[0] = %u, expected 0", rp[0]);
-    for (int64_t i = 0; i < n; ++i)
-        if (rp[i + 1] < rp[i]) return fail(OHM_ERR_COMPILE, "row_ptr decreases at row %lld", (long long)i);
-    if ((int64_t)rp[n] != nnz) return fail(OHM_ERR_COMPILE, "row_ptr[n] = %u != nnz %lld", rp[n], (long long)nnz);
-    for (int64_t k = 0; k < nnz; ++k)
-        if ((int64_t)col[k] >= n) return fail(OHM_ERR_COMPILE, "column index %u out of range at %lld", col[k], (long long)k);
-    return OHM_OK;
-}
-
-static inline bool idx_ok(uint32_t v, int64_t lim) { return v == kSentinel || (int64_t)v < lim; }
-
-static ohm_status check_devices(const ohm_diode_desc *d, int64_t nd, const ohm_bjt_desc *q, int64_t nq,
-                                const ohm_mosfet_desc *m, int64_t nm, int64_t size, int64_t nnz) {
-    if (nd < 0 || nq < 0 || nm < 0) return fail(OHM_ERR_INVALID_ARG, "negative device count");
-    if ((nd && !d) || (nq && !q) || (nm && !m)) return fail(OHM_ERR_INVALID_ARG, "null descriptor array");
-    for (int64_t k = 0; k < nd; ++k) {
-        const ohm_diode_desc &x = d[k];
-        bool ok = idx_ok(x.anode_idx, size) && idx_ok(x.cathode_idx, size);
-        for (int j = 0; j < 4; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
-        for (int j = 0; j < 2; ++j) ok = ok && idx_ok(x.b_idx[j], size);
-        if (!ok) return fail(OHM_ERR_COMPILE, "diode %lld has an index out of range", (long long)k);
-    }
-    for (int64_t k = 0; k < nq; ++k) {
-        const ohm_bjt_desc &x = q[k];
-        bool ok = idx_ok(x.collector_idx, size) && idx_ok(x.base_idx, size) && idx_ok(x.emitter_idx, size);
-        for (int j = 0; j < 9; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
-        for (int j = 0; j < 3; ++j) ok = ok && idx_ok(x.b_idx[j], size);
-        if (!ok) return fail(OHM_ERR_COMPILE, "BJT %lld has an index out of range", (long long)k);
-    }
-    for (int64_t k = 0; k < nm; ++k) {
-        const ohm_mosfet_desc &x = m[k];
-        bool ok = idx_ok(x.drain_idx, size) && idx_ok(x.gate_idx, size) && idx_ok(x.source_idx, size);
-        for (int j = 0; j < 6; ++j) ok = ok && idx_ok(x.g_row_col[j], nnz);
-        for (int j = 0; j < 2; ++j) ok = ok && idx_ok(x.b_idx[j], size);
-        if (!ok) return fail(OHM_ERR_COMPILE, "MOSFET %lld has an index out of range", (long long)k);
-    }
-    return OHM_OK;
-}
-
-// --------------------------------------------------- preconditioner setup --
-// Block-Jacobi structure.  Rows whose diagonal is structurally zero (voltage
-// source and inductor branch rows of an MNA matrix, src/compiler.rs:376-408)
-// are paired with the off-diagonal column of largest magnitude whose row is
-// unpaired and has a usable diagonal; the 2x2 block [[a_jj a_jk][a_kj 0]] has
-// det = -a_jk a_kj != 0.  Unpaired zero-diagonal rows keep the reference's
-// Jacobi rule (inverse 0).  `touched` marks diagonal slots the device stamps
-// change; those rows never count as zero-diagonal.
-struct PcHost {
-    std::vector<int32_t> partner;
-    std::vector<uint32_t> diag_slot, off_slot;
-    std::vector<uint8_t> rowflag;   // row or one of its columns is paired
-    bool any_pair = false;
-};
-
-static void build_precond(int64_t n, const uint32_t *rp, const uint32_t *col, const double *val,
-                          const std::vector<char> &touched_slot, bool pairs, PcHost &pc) {
-    pc.partner.assign(n, -1);
-    pc.diag_slot.assign(n, kSentinel);
-    pc.off_slot.assign(n, kSentinel);
-    pc.rowflag.clear();
-    pc.any_pair = false;
-    for (int64_t i = 0; i < n; ++i)
-        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
-            if ((int64_t)col[k] == i) { pc.diag_slot[i] = k; break; }
-    if (!pairs) {
-        pc.rowflag.assign(n, 0);
-        return;
-    }
-    auto zero_diag = [&](int64_t i) {
-        const uint32_t s = pc.diag_slot[i];
-        if (s == kSentinel) return true;
-        if (!touched_slot.empty() && touched_slot[s]) return false;
-        return std::fabs(val[s]) <= 1e-30;
-    };
-    auto slot_of = [&](int64_t r, int64_t c) -> uint32_t {
-        for (uint32_t k = rp[r]; k < rp[r + 1]; ++k)
-            if ((int64_t)col[k] == c) return k;
-        return kSentinel;
-    };
-    for (int64_t k = 0; k < n; ++k) {
-        if (!zero_diag(k) || pc.partner[k] >= 0) continue;
-        int64_t best = -1;
-        double best_mag = 0.0;
-        uint32_t best_kj = kSentinel, best_jk = kSentinel;
-        for (uint32_t e = rp[k]; e < rp[k + 1]; ++e) {
-            const int64_t j = col[e];
-            if (j == k || pc.partner[j] >= 0 || zero_diag(j)) continue;
-            const double mag = std::fabs(val[e]);
-            if (!(mag > 0.0)) continue;
-            const uint32_t jk = slot_of(j, k);
-            if (jk == kSentinel || !(std::fabs(val[jk]) > 0.0)) continue;
-            if (mag > best_mag) { best_mag = mag; best = j; best_kj = e; best_jk = jk; }
-        }
-        if (best >= 0) {
-            pc.partner[k] = (int32_t)best;
-            pc.partner[best] = (int32_t)k;
-            pc.off_slot[k] = best_kj;
-            pc.off_slot[best] = best_jk;
-            pc.any_pair = true;
-        }
-    }
-    pc.rowflag.assign(n, 0);
-    if (pc.any_pair)
-        for (int64_t i = 0; i < n; ++i) {
-            bool f = pc.partner[i] >= 0;
-            for (uint32_t k = rp[i]; k < rp[i + 1] && !f; ++k) f = pc.partner[col[k]] >= 0;
-            pc.rowflag[i] = f ? 1 : 0;
-        }
-}
 
 // ------------------------------------------------------------ launch logic --
 using KernelFn = void (*)(KernelArgs);
@@ -628,25 +514,6 @@ static void plan_free(ohm_plan *p) {
     delete p;
 }
 
-// Stamp map: every (slot, contribution id) pair, grouped by slot.  Ids are
-// assigned diodes first, then BJTs, then MOSFETs, device-major, so each slot
-// sums its contributions in that fixed (canonical) order.
-static void build_stamp_map(const std::vector<std::pair<uint32_t, uint32_t>> &pairs_in,
-                            std::vector<uint32_t> &slots, std::vector<uint32_t> &ptr, std::vector<uint32_t> &ids) {
-    std::vector<std::pair<uint32_t, uint32_t>> pairs(pairs_in);
-    std::stable_sort(pairs.begin(), pairs.end(),
-                     [](const auto &x, const auto &y) { return x.first < y.first; });
-    slots.clear(); ptr.clear(); ids.clear();
-    for (size_t k = 0; k < pairs.size(); ++k) {
-        if (k == 0 || pairs[k].first != pairs[k - 1].first) {
-            slots.push_back(pairs[k].first);
-            ptr.push_back((uint32_t)ids.size());
-        }
-        ids.push_back(pairs[k].second);
-    }
-    ptr.push_back((uint32_t)ids.size());
-}
-
 template <typename T>
 static cudaError_t up(T **dst, const T *src, size_t count, cudaStream_t s) {
     cudaError_t e = dalloc(dst, count);
@@ -879,6 +746,71 @@ extern "C" ohm_status ohm_newton_solve(ohm_ctx *c, const double *base_g_values, 
         if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "download: %s", cudaGetErrorString(e));
     }
     ohm_plan_destroy(p);
+    return st;
+}
+
+// ---------------------------------------------------------- ISAI(1) hook --
+// One block builds the ILU(0) factor and the ISAI(1) columns (the same
+// isai_setup the solver runs) and applies z = M_U (M_L r) to each vector.
+__global__ void __launch_bounds__(1024) isai_apply_kernel(KernelArgs a, const double *R, double *Z, double *Y,
+                                                          int n_vec) {
+    __shared__ double smem[32 * 4];
+    BlockTeam g;
+    g.r0 = 0; g.r1 = a.n; g.gtid = threadIdx.x; g.gstride = blockDim.x; g.smem = smem;
+    if (!isai_setup(a, g)) return;
+    const int n = a.n;
+    for (int v = 0; v < n_vec; ++v) {
+        const double *r = R + (size_t)v * n;
+        double *z = Z + (size_t)v * n;
+        spmv_rows<1, double>(a.ml_rp, a.ml_col, a.ml_val, (const uint8_t *)nullptr, 0, n,
+                             [&](int j, bool) { return r[j]; }, [&](int i, double y) { Y[i] = y; });
+        __syncthreads();
+        spmv_rows<1, double>(a.mu_rp, a.mu_col, a.mu_val, (const uint8_t *)nullptr, 0, n,
+                             [&](int j, bool) { return Y[j]; }, [&](int i, double y) { z[i] = y; });
+        __syncthreads();
+    }
+}
+
+extern "C" ohm_status ohm_isai_apply(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *row_ptr, const uint32_t *col,
+                                     const double *values, const double *r, double *z, int64_t n_vectors) {
+    if (!c) return fail(OHM_ERR_INVALID_ARG, "ctx is null");
+    if (n <= 0 || n_vectors < 0 || !r || !z || (nnz && !values)) return fail(OHM_ERR_INVALID_ARG, "bad arguments");
+    if (n * std::max<int64_t>(n_vectors, 1) > (int64_t)1 << 28) return fail(OHM_ERR_INVALID_ARG, "too many vectors");
+    ohm_status st = check_csr(n, nnz, row_ptr, col);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaSetDevice(c->device));
+    IsaiDev isai;
+    uint32_t *d_rp = nullptr, *d_col = nullptr;
+    double *d_val = nullptr, *d_r = nullptr, *d_z = nullptr, *d_y = nullptr;
+    const size_t nv = (size_t)n * (size_t)n_vectors;
+    cudaError_t e = isai.build(n, row_ptr, col, c->stream);
+    if (e == cudaSuccess) e = dalloc(&d_rp, n + 1);
+    if (e == cudaSuccess) e = dalloc(&d_col, nnz);
+    if (e == cudaSuccess) e = dalloc(&d_val, nnz);
+    if (e == cudaSuccess) e = dalloc(&d_r, nv);
+    if (e == cudaSuccess) e = dalloc(&d_z, nv);
+    if (e == cudaSuccess) e = dalloc(&d_y, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rp, row_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_col, col, nnz * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_val, values, nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nv) e = cudaMemcpyAsync(d_r, r, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        KernelArgs a{};
+        a.n = (int)n;
+        a.nnz = (int)nnz;
+        a.row_ptr = d_rp;
+        a.col = d_col;
+        a.vals64 = d_val;
+        isai.bind(a);
+        isai_apply_kernel<<<1, 1024, 0, c->stream>>>(a, d_r, d_z, d_y, (int)n_vectors);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && nv) e = cudaMemcpyAsync(z, d_z, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "isai apply: %s", cudaGetErrorString(e));
+    cudaStreamSynchronize(c->stream);
+    cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_r); cudaFree(d_z); cudaFree(d_y);
+    isai.release();
     return st;
 }
 

@@ -1,0 +1,413 @@
+// Batched Newton: many independent circuits (Monte Carlo corners, parameter
+// sweeps) solved by one launch.  Each block takes circuits from a work queue
+// in decreasing order of nonzeros (longest-processing-time first) and runs the
+// complete Newton loop of solve_body on it with block-level synchronisation
+// only, so blocks never wait on each other.  The systems are stored packed:
+// block-diagonal CSR with per-circuit local indices and offset tables.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "host_util.h"
+
+using namespace ohm;
+
+namespace {
+
+constexpr int kBatchBlock = 256;
+
+struct BatchArgs {
+    KernelArgs base;                // pointers to the packed arrays, shared scalars
+    int n_inst;
+    const int64_t *row_off, *nnz_off;
+    const int64_t *d_off, *q_off, *m_off;      // device descriptor offsets
+    const int64_t *ms_off, *mid_off, *rs_off, *rid_off;   // stamp-map offsets
+    const int32_t *order;           // instances by decreasing nnz
+    unsigned int *queue;            // next position in `order`
+    DeviceInfo *infos;              // per instance
+    double *node_scale_base;        // per row (8 bytes)
+};
+
+template <typename P>
+__device__ __forceinline__ P *offset(P *p, int64_t k) { return p ? p + k : p; }
+
+template <int LPR>
+__global__ void __launch_bounds__(kBatchBlock) batch_solver(BatchArgs B) {
+    __shared__ double smem[32 * 4];
+    __shared__ int s_q;
+    for (;;) {
+        if (threadIdx.x == 0) s_q = (int)atomicAdd(B.queue, 1u);
+        __syncthreads();
+        const int q = s_q;
+        __syncthreads();
+        if (q >= B.n_inst) return;
+        const int i = B.order[q];
+        const int64_t ro = B.row_off[i], no = B.nnz_off[i];
+        const int64_t dq = B.d_off[i], qq = B.q_off[i], mq = B.m_off[i];
+        KernelArgs a = B.base;
+        a.n = (int)(B.row_off[i + 1] - ro);
+        a.nnz = (int)(B.nnz_off[i + 1] - no);
+        a.row_ptr = B.base.row_ptr + ro + i;               // n_i + 1 local row pointers
+        a.col = B.base.col + no;
+        a.vals64 = B.base.vals64 + no;
+        a.vals32 = offset(B.base.vals32, no);
+        a.base_vals = B.base.base_vals + no;
+        a.base_b = B.base.base_b + ro;
+        a.b = B.base.b + ro;
+        a.x = B.base.x + ro;
+        a.x_prev = B.base.x_prev + ro;
+        a.r64 = B.base.r64 + ro;
+        a.dx = B.base.dx + ro;
+        a.partner = B.base.partner + ro;
+        a.diag_slot = B.base.diag_slot + ro;
+        a.off_slot = B.base.off_slot + ro;
+        a.rowflag = offset(B.base.rowflag, ro);
+        a.pc_part = (double *)B.base.pc_part + ro;
+        a.rec0 = (double *)B.base.rec0 + 4 * ro;
+        a.rec1 = (double *)B.base.rec1 + 4 * ro;
+        a.rhat = (double *)B.base.rhat + ro;
+        a.s = (double *)B.base.s + ro;
+        a.t = (double *)B.base.t + ro;
+        a.phat = (double *)B.base.phat + ro;
+        a.shat = (double *)B.base.shat + ro;
+        a.d = (double *)B.base.d + ro;
+        a.nd = (int)(B.d_off[i + 1] - dq);
+        a.nq = (int)(B.q_off[i + 1] - qq);
+        a.nm = (int)(B.m_off[i + 1] - mq);
+        a.diodes = B.base.diodes + dq;
+        a.bjts = B.base.bjts + qq;
+        a.mosfets = B.base.mosfets + mq;
+        a.bjt_vaf = offset(B.base.bjt_vaf, qq);
+        a.mstamp = B.base.mstamp + 4 * dq + 9 * qq + 6 * mq;
+        a.rstamp = B.base.rstamp + 2 * dq + 3 * qq + 2 * mq;
+        a.n_mslots = (int)(B.ms_off[i + 1] - B.ms_off[i]);
+        a.mslot = B.base.mslot + B.ms_off[i];
+        a.mslot_ptr = B.base.mslot_ptr + B.ms_off[i] + i;
+        a.mslot_ids = B.base.mslot_ids + B.mid_off[i];
+        a.n_rrows = (int)(B.rs_off[i + 1] - B.rs_off[i]);
+        a.rrow = B.base.rrow + B.rs_off[i];
+        a.rrow_ptr = B.base.rrow_ptr + B.rs_off[i] + i;
+        a.rrow_ids = B.base.rrow_ids + B.rid_off[i];
+        a.node_scale = (unsigned long long *)(B.node_scale_base + ro);
+        a.trace = nullptr;
+        BlockTeam g;
+        g.r0 = 0;
+        g.r1 = a.n;
+        g.gtid = threadIdx.x;
+        g.gstride = blockDim.x;
+        g.smem = smem;
+        solve_body<LPR>(a, g, &B.infos[i]);
+        __syncthreads();
+    }
+}
+
+using BatchFn = void (*)(BatchArgs);
+
+BatchFn pick(int lpr) {
+    switch (lpr) {
+        case 1: return batch_solver<1>;
+        case 2: return batch_solver<2>;
+        case 4: return batch_solver<4>;
+        case 8: return batch_solver<8>;
+        default: return batch_solver<16>;
+    }
+}
+
+}  // namespace
+
+struct ohm_batch {
+    ohm_ctx *ctx = nullptr;
+    int64_t n_inst = 0, rows = 0, nnz = 0, nd = 0, nq = 0, nm = 0;
+    int lpr = 2;
+    std::vector<void *> allocs;
+    BatchArgs args{};
+    std::vector<DeviceInfo> host_infos;
+    DeviceInfo *infos = nullptr;
+    unsigned int *queue = nullptr;
+
+    template <typename T>
+    cudaError_t put(T **dst, const T *src, size_t count) {
+        cudaError_t e = dalloc(dst, count);
+        if (e == cudaSuccess) allocs.push_back((void *)*dst);
+        if (e == cudaSuccess && src && count)
+            e = cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+        return e;
+    }
+    template <typename T>
+    cudaError_t zero(T **dst, size_t count) {
+        cudaError_t e = put(dst, (const T *)nullptr, count);
+        if (e == cudaSuccess) e = cudaMemsetAsync(*dst, 0, std::max<size_t>(count, 1) * sizeof(T), ctx->stream);
+        return e;
+    }
+};
+
+extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t *row_off, const int64_t *nnz_off,
+                                       const uint32_t *row_ptrs, const uint32_t *col_indices,
+                                       const double *base_g_values, const double *base_b,
+                                       const int64_t *diode_off, const ohm_diode_desc *diodes,
+                                       const int64_t *bjt_off, const ohm_bjt_desc *bjts, const double *bjt_vaf,
+                                       const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets, ohm_batch **out) {
+    if (!c || !out || n_inst <= 0 || !row_off || !nnz_off || !row_ptrs || !base_g_values || !base_b ||
+        !diode_off || !bjt_off || !mosfet_off)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "bad batch arguments");
+    *out = nullptr;
+    if (row_off[0] != 0 || nnz_off[0] != 0 || diode_off[0] != 0 || bjt_off[0] != 0 || mosfet_off[0] != 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "offset tables must start at 0");
+    const int64_t rows = row_off[n_inst], nnz = nnz_off[n_inst];
+    const int64_t nd = diode_off[n_inst], nq = bjt_off[n_inst], nm = mosfet_off[n_inst];
+    if ((nnz && !col_indices) || (nd && !diodes) || (nq && !bjts) || (nm && !mosfets))
+        return ohm_fail(OHM_ERR_INVALID_ARG, "null packed array");
+    if (rows > 0x7fffffffLL || nnz > 0x7fffffffLL) return ohm_fail(OHM_ERR_INVALID_ARG, "batch too large");
+    CUDA_TRY(cudaSetDevice(c->device));
+
+    // per-instance validation, stamp maps and preconditioner structure (local indices)
+    std::vector<int64_t> ms_off(n_inst + 1, 0), mid_off(n_inst + 1, 0), rs_off(n_inst + 1, 0), rid_off(n_inst + 1, 0);
+    std::vector<uint32_t> mslot, mptr, mids, rrow, rptr, rids;
+    std::vector<int32_t> partner(rows);
+    std::vector<uint32_t> diag(rows), off(rows);
+    std::vector<uint8_t> flag(rows);
+    bool any_pair = false;
+    int64_t max_nnz_row = 0;
+    for (int64_t i = 0; i < n_inst; ++i) {
+        const int64_t n = row_off[i + 1] - row_off[i], z = nnz_off[i + 1] - nnz_off[i];
+        if (n <= 0 || z < 0) return ohm_fail(OHM_ERR_INVALID_ARG, "instance %lld has no rows", (long long)i);
+        const uint32_t *rp = row_ptrs + row_off[i] + i;
+        const uint32_t *cl = col_indices + nnz_off[i];
+        ohm_status st = check_csr(n, z, rp, cl);
+        if (st != OHM_OK) return ohm_fail(st, "instance %lld: %s", (long long)i, ohm_last_error());
+        const ohm_diode_desc *d = diodes + diode_off[i];
+        const ohm_bjt_desc *q = bjts + bjt_off[i];
+        const ohm_mosfet_desc *m = mosfets + mosfet_off[i];
+        const int64_t dn = diode_off[i + 1] - diode_off[i], qn = bjt_off[i + 1] - bjt_off[i],
+                      mn = mosfet_off[i + 1] - mosfet_off[i];
+        st = check_devices(d, dn, q, qn, m, mn, n, z);
+        if (st != OHM_OK) return ohm_fail(st, "instance %lld: %s", (long long)i, ohm_last_error());
+        std::vector<std::pair<uint32_t, uint32_t>> mp, rp_;
+        const uint32_t bq = 4u * (uint32_t)dn, bm = bq + 9u * (uint32_t)qn;
+        const uint32_t rbq = 2u * (uint32_t)dn, rbm = rbq + 3u * (uint32_t)qn;
+        for (int64_t k = 0; k < dn; ++k) {
+            for (int j = 0; j < 4; ++j) if (d[k].g_row_col[j] != kSentinel) mp.push_back({d[k].g_row_col[j], (uint32_t)(4 * k + j)});
+            for (int j = 0; j < 2; ++j) if (d[k].b_idx[j] != kSentinel) rp_.push_back({d[k].b_idx[j], (uint32_t)(2 * k + j)});
+        }
+        for (int64_t k = 0; k < qn; ++k) {
+            for (int j = 0; j < 9; ++j) if (q[k].g_row_col[j] != kSentinel) mp.push_back({q[k].g_row_col[j], bq + (uint32_t)(9 * k + j)});
+            for (int j = 0; j < 3; ++j) if (q[k].b_idx[j] != kSentinel) rp_.push_back({q[k].b_idx[j], rbq + (uint32_t)(3 * k + j)});
+        }
+        for (int64_t k = 0; k < mn; ++k) {
+            for (int j = 0; j < 6; ++j) if (m[k].g_row_col[j] != kSentinel) mp.push_back({m[k].g_row_col[j], bm + (uint32_t)(6 * k + j)});
+            for (int j = 0; j < 2; ++j) if (m[k].b_idx[j] != kSentinel) rp_.push_back({m[k].b_idx[j], rbm + (uint32_t)(2 * k + j)});
+        }
+        std::vector<uint32_t> s1, p1, i1, s2, p2, i2;
+        build_stamp_map(mp, s1, p1, i1);
+        build_stamp_map(rp_, s2, p2, i2);
+        ms_off[i + 1] = ms_off[i] + (int64_t)s1.size();
+        mid_off[i + 1] = mid_off[i] + (int64_t)i1.size();
+        rs_off[i + 1] = rs_off[i] + (int64_t)s2.size();
+        rid_off[i + 1] = rid_off[i] + (int64_t)i2.size();
+        mslot.insert(mslot.end(), s1.begin(), s1.end());
+        mptr.insert(mptr.end(), p1.begin(), p1.end());       // s1.size()+1 entries
+        mids.insert(mids.end(), i1.begin(), i1.end());
+        rrow.insert(rrow.end(), s2.begin(), s2.end());
+        rptr.insert(rptr.end(), p2.begin(), p2.end());
+        rids.insert(rids.end(), i2.begin(), i2.end());
+        std::vector<char> touched(z, 0);
+        for (uint32_t sl : s1) touched[sl] = 1;
+        PcHost pc;
+        build_precond(n, rp, cl, base_g_values + nnz_off[i], touched, true, pc);
+        std::copy(pc.partner.begin(), pc.partner.end(), partner.begin() + row_off[i]);
+        std::copy(pc.diag_slot.begin(), pc.diag_slot.end(), diag.begin() + row_off[i]);
+        std::copy(pc.off_slot.begin(), pc.off_slot.end(), off.begin() + row_off[i]);
+        std::copy(pc.rowflag.begin(), pc.rowflag.end(), flag.begin() + row_off[i]);
+        any_pair |= pc.any_pair;
+        for (int64_t r = 0; r < n; ++r) max_nnz_row = std::max<int64_t>(max_nnz_row, rp[r + 1] - rp[r]);
+    }
+    // longest first
+    std::vector<int32_t> order(n_inst);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+        return (nnz_off[x + 1] - nnz_off[x]) > (nnz_off[y + 1] - nnz_off[y]);
+    });
+
+    ohm_batch *b = new ohm_batch();
+    b->ctx = c;
+    b->n_inst = n_inst; b->rows = rows; b->nnz = nnz; b->nd = nd; b->nq = nq; b->nm = nm;
+    const double avg = (double)nnz / (double)rows;
+    b->lpr = avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : (avg <= 24.0 ? 8 : 16)));
+    KernelArgs &a = b->args.base;
+    a = KernelArgs{};
+    uint32_t *u32 = nullptr;
+    double *f64 = nullptr;
+    cudaError_t e = cudaSuccess;
+#define PUT(dst, src, cnt) do { if (e == cudaSuccess) e = b->put(&(dst), (src), (cnt)); } while (0)
+#define ZERO(dst, cnt) do { if (e == cudaSuccess) e = b->zero(&(dst), (cnt)); } while (0)
+    PUT(u32, row_ptrs, rows + n_inst); a.row_ptr = u32;
+    PUT(u32, col_indices, nnz); a.col = u32;
+    PUT(f64, base_g_values, nnz); a.base_vals = f64;
+    PUT(f64, base_g_values, nnz); a.vals64 = f64;
+    float *v32 = nullptr; ZERO(v32, nnz); a.vals32 = v32;
+    PUT(f64, base_b, rows); a.base_b = f64;
+    PUT(f64, base_b, rows); a.b = f64;
+    ZERO(f64, rows); a.x_prev = f64;
+    ZERO(f64, rows); a.r64 = f64;
+    ZERO(f64, rows); a.dx = f64;
+    ZERO(f64, rows); b->args.node_scale_base = f64;
+    int32_t *i32 = nullptr;
+    PUT(i32, partner.data(), rows); a.partner = i32;
+    PUT(u32, diag.data(), rows); a.diag_slot = u32;
+    PUT(u32, off.data(), rows); a.off_slot = u32;
+    uint8_t *u8 = nullptr;
+    if (any_pair) { PUT(u8, flag.data(), rows); a.rowflag = u8; }
+    ZERO(f64, 4 * rows); a.rec0 = f64;
+    ZERO(f64, 4 * rows); a.rec1 = f64;
+    void **vs[] = {&a.rhat, &a.s, &a.t, &a.phat, &a.shat, &a.d, &a.pc_part};
+    for (void **slot : vs) { ZERO(f64, rows); *slot = f64; }
+    DiodeDesc *dd = nullptr; PUT(dd, (const DiodeDesc *)diodes, nd); a.diodes = dd;
+    BjtDesc *qd = nullptr; PUT(qd, (const BjtDesc *)bjts, nq); a.bjts = qd;
+    MosfetDesc *md = nullptr; PUT(md, (const MosfetDesc *)mosfets, nm); a.mosfets = md;
+    if (bjt_vaf && nq) { PUT(f64, bjt_vaf, nq); a.bjt_vaf = f64; }
+    ZERO(f64, 4 * nd + 9 * nq + 6 * nm); a.mstamp = f64;
+    ZERO(f64, 2 * nd + 3 * nq + 2 * nm); a.rstamp = f64;
+    PUT(u32, mslot.data(), mslot.size()); a.mslot = u32;
+    PUT(u32, mptr.data(), mptr.size()); a.mslot_ptr = u32;
+    PUT(u32, mids.data(), mids.size()); a.mslot_ids = u32;
+    PUT(u32, rrow.data(), rrow.size()); a.rrow = u32;
+    PUT(u32, rptr.data(), rptr.size()); a.rrow_ptr = u32;
+    PUT(u32, rids.data(), rids.size()); a.rrow_ids = u32;
+    int64_t *i64 = nullptr;
+    PUT(i64, row_off, n_inst + 1); b->args.row_off = i64;
+    PUT(i64, nnz_off, n_inst + 1); b->args.nnz_off = i64;
+    PUT(i64, diode_off, n_inst + 1); b->args.d_off = i64;
+    PUT(i64, bjt_off, n_inst + 1); b->args.q_off = i64;
+    PUT(i64, mosfet_off, n_inst + 1); b->args.m_off = i64;
+    PUT(i64, ms_off.data(), n_inst + 1); b->args.ms_off = i64;
+    PUT(i64, mid_off.data(), n_inst + 1); b->args.mid_off = i64;
+    PUT(i64, rs_off.data(), n_inst + 1); b->args.rs_off = i64;
+    PUT(i64, rid_off.data(), n_inst + 1); b->args.rid_off = i64;
+    PUT(i32, order.data(), n_inst); b->args.order = i32;
+    ZERO(b->infos, n_inst);
+    ZERO(b->queue, 4);
+#undef PUT
+#undef ZERO
+    if (e == cudaSuccess && nnz) e = ohm_f64_to_f32(a.vals64, v32, nnz, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);   // host vectors go out of scope
+    if (e != cudaSuccess) {
+        for (void *p : b->allocs) cudaFree(p);
+        delete b;
+        return ohm_fail(OHM_ERR_CUDA, "batch upload: %s", cudaGetErrorString(e));
+    }
+    b->args.n_inst = (int)n_inst;
+    b->args.infos = b->infos;
+    b->args.queue = b->queue;
+    b->host_infos.resize(n_inst);
+    ohm_ctx_retain(c);
+    *out = b;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_destroy(ohm_batch *b) {
+    if (!b) return OHM_OK;
+    ohm_ctx *c = b->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (void *p : b->allocs) cudaFree(p);
+    delete b;
+    ohm_ctx_release(c);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const ohm_newton_params *np,
+                                              ohm_solve_info *summary) {
+    if (!b || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (np->max_iterations <= 0) return ohm_fail(OHM_ERR_NEWTON_NOT_CONVERGED, "Newton solver did not converge after 0 iterations");
+    ohm_status st = ohm_check_krylov(&np->krylov);
+    if (st != OHM_OK) return st;
+    if (np->krylov.precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "batched solves use block Jacobi (ISAI(1) is for single systems)");
+    ohm_ctx *c = b->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    BatchArgs B = b->args;
+    KernelArgs &a = B.base;
+    a.x = x_dev;
+    a.precond = np->krylov.precond == OHM_PRECOND_NONE ? kPcNone
+              : (np->krylov.precond == OHM_PRECOND_JACOBI ? kPcJacobi : kPcAuto);
+    if (a.precond != kPcAuto) a.rowflag = nullptr;
+    a.newton = 1;
+    const bool mixed = np->krylov.precision == OHM_PREC_MIXED;
+    a.mixed = mixed ? 1 : 0;
+    a.max_outer = np->max_iterations;
+    a.abs_tol = np->abs_tol;
+    a.rel_tol = np->rel_tol;
+    a.max_krylov = np->krylov.max_iterations;
+    a.krylov_tol = np->krylov.tolerance;
+    a.inner_rtol = mixed ? (np->krylov.inner_rtol > 0.0 ? np->krylov.inner_rtol : 1e-4) : np->krylov.inner_rtol;
+    a.forcing = np->forcing;
+    a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
+    a.fp32_max_iterations = np->krylov.fp32_max_iterations > 0 ? np->krylov.fp32_max_iterations
+                                                               : np->krylov.max_iterations;
+    a.max_restarts = std::max(0, np->krylov.max_restarts);
+    if (np->initial_guess)
+        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, b->rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(b->infos, 0, b->n_inst * sizeof(DeviceInfo), c->stream));
+    BatchFn fn = pick(b->lpr);
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchBlock, 0));
+    if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "batch kernel does not fit on an SM");
+    const int grid = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, b->n_inst);
+    fn<<<grid, kBatchBlock, 0, c->stream>>>(B);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(b->host_infos.data(), b->infos, b->n_inst * sizeof(DeviceInfo), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // summary: worst status, totals
+    int64_t kit = 0, fb = 0, rs = 0, worst = -1;
+    int max_newton = 0;
+    for (int64_t i = 0; i < b->n_inst; ++i) {
+        const DeviceInfo &d = b->host_infos[i];
+        kit += d.krylov_iterations;
+        fb += d.fp64_fallbacks;
+        rs += d.krylov_restarts;
+        max_newton = std::max(max_newton, d.iterations);
+        if (d.status != 0 && worst < 0) worst = i;
+    }
+    if (summary) {
+        std::memset(summary, 0, sizeof *summary);
+        summary->iterations = max_newton;
+        summary->krylov_iterations = kit;
+        summary->fp64_fallbacks = (int32_t)fb;
+        summary->krylov_restarts = (int32_t)rs;
+        summary->kernel_launches = 1;
+        summary->status = worst < 0 ? OHM_OK : b->host_infos[worst].status;
+        summary->error_iteration = (int32_t)worst;
+    }
+    if (worst >= 0) {
+        const DeviceInfo &d = b->host_infos[worst];
+        return ohm_fail(d.status == 1 ? OHM_ERR_SOLVE : (d.status == 3 ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
+                        "instance %lld failed: status %d (krylov code %d) after %d Newton iterations",
+                        (long long)worst, d.status, d.krylov_code, d.iterations);
+    }
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_instance_info(ohm_batch *b, ohm_solve_info *infos, int64_t n) {
+    if (!b || !infos || n != b->n_inst) return ohm_fail(OHM_ERR_INVALID_ARG, "bad arguments");
+    for (int64_t i = 0; i < n; ++i) {
+        const DeviceInfo &d = b->host_infos[i];
+        ohm_solve_info &o = infos[i];
+        std::memset(&o, 0, sizeof o);
+        o.status = d.status == 0 ? OHM_OK : (d.status == 1 ? OHM_ERR_SOLVE : (d.status == 3 ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED));
+        o.krylov_code = d.krylov_code;
+        o.iterations = d.iterations;
+        o.error_iteration = d.error_iteration;
+        o.krylov_iterations = d.krylov_iterations;
+        o.fp64_fallbacks = d.fp64_fallbacks;
+        o.krylov_restarts = d.krylov_restarts;
+        o.max_residual = d.max_residual;
+        o.b_norm = d.b_norm;
+        o.kernel_launches = 1;
+    }
+    return OHM_OK;
+}

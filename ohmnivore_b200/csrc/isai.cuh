@@ -15,7 +15,8 @@ constexpr int kIsaiLocal = 32;
 // fill (factor initial guess from A), kChowPatelSweeps fixed-point sweeps
 // (Jacobi style, double-buffered, so the result is deterministic), then one
 // thread per column of M_L and of M_U.  Returns false if a barrier gave up.
-__device__ __forceinline__ bool isai_setup(const KernelArgs &a, Grid &g) {
+template <class Team>
+__device__ __forceinline__ bool isai_setup(const KernelArgs &a, Team &g) {
     const int n = a.n;
     const int gtid = g.gtid, gstride = g.gstride;
     double *F = a.isai_f0, *Fn = a.isai_f1;
@@ -34,7 +35,7 @@ __device__ __forceinline__ bool isai_setup(const KernelArgs &a, Grid &g) {
             }
         }
     }
-    if (!grid_barrier(g.gs, g.epoch)) return false;
+    if (!g.sync()) return false;
     for (int sweep = 0; sweep < kChowPatelSweeps; ++sweep) {
         for (int i = gtid; i < n; i += gstride) {
             for (uint32_t s = a.aug_rp[i]; s < a.aug_rp[i + 1]; ++s) {
@@ -50,7 +51,7 @@ __device__ __forceinline__ bool isai_setup(const KernelArgs &a, Grid &g) {
                 Fn[s] = acc;
             }
         }
-        if (!grid_barrier(g.gs, g.epoch)) return false;
+        if (!g.sync()) return false;
         double *tmp = F; F = Fn; Fn = tmp;
     }
     // value of the factor at (r, c): L (strict lower, unit diagonal implied) or U
@@ -90,15 +91,15 @@ __device__ __forceinline__ bool isai_setup(const KernelArgs &a, Grid &g) {
             }
         }
     }
-    return grid_barrier(g.gs, g.epoch);
+    return g.sync();
 }
 
 // Right-preconditioned BiCGSTAB with the ISAI(1) apply, same operation order
 // as krylov() (bicgstab.rs:104-183); seven grid synchronisations per
 // iteration: y = M_L p (p formed on the fly), phat = M_U y, v = A phat,
 // y = M_L s (s formed on the fly), shat = M_U y, t = A shat, update.
-template <typename T, int LPR>
-__device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
+template <typename T, int LPR, class Team>
+__device__ __forceinline__ int krylov_isai(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                            int max_it, bool accept_partial, KrylovOut &out) {
     using Acc = T;
     const int r0 = g.r0, r1 = g.r1, n = a.n;
@@ -119,10 +120,7 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double 
         acc0[0] += (double)rt * (double)rt;
     }
     {
-        double *pr = g.part();
-        publish_partials<1>(acc0, pr, g.smem);
-        OHM_SYNC_OR(kKrylovAbort);
-        gather_partials<1>(pr, acc0, g.smem);
+        if (!g.template allreduce<1>(acc0)) return kKrylovAbort;
     }
     const double r0norm = sqrt(acc0[0]);
     const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
@@ -180,10 +178,7 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double 
                 acc1[1] += (double)vt * (double)vt;
             });
             {
-                double *pr = g.part();
-                publish_partials<2>(acc1, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc1, g.smem);
+                if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
             }
             if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
@@ -206,10 +201,7 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double 
                                        acc2[0] += (double)si * (double)si;
                                    });
             {
-                double *pr = g.part();
-                publish_partials<1>(acc2, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<1>(pr, acc2, g.smem);
+                if (!g.template allreduce<1>(acc2)) return kKrylovAbort;
             }
             if (sqrt(acc2[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
@@ -232,10 +224,7 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double 
                 acc3[1] += (double)tt * (double)tt;
             });
             {
-                double *pr = g.part();
-                publish_partials<2>(acc3, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc3, g.smem);
+                if (!g.template allreduce<2>(acc3)) return kKrylovAbort;
             }
             if (!(acc3[1] > 0.0)) { code = kKrylovBreakTt; break; }
             omega = acc3[0] / acc3[1];
@@ -248,10 +237,7 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Grid &g, double 
                 acc4[1] += (double)rt * (double)rt;
             }
             {
-                double *pr = g.part();
-                publish_partials<2>(acc4, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc4, g.smem);
+                if (!g.template allreduce<2>(acc4)) return kKrylovAbort;
             }
             rho_new = acc4[0];
             rr_cur = acc4[1];

@@ -158,8 +158,12 @@ struct KernelArgs {
 // used, max|x - x_old| after limiting, restarts.
 constexpr int kTraceCols = 6;
 
-// Per-block view of the launch: row range, barrier epoch, reduction buffers.
-struct Grid {
+// A team is the set of threads that solves one system: the whole grid (one
+// large circuit, GridTeam) or one block (one circuit of a batch, BlockTeam).
+// Both expose the rows this block owns [r0, r1), a thread index / stride over
+// the team for device- and slot-parallel loops, sync() and deterministic
+// all-reductions whose results are bit-identical in every thread.
+struct GridTeam {
     int G, bid, r0, r1, gtid, gstride;
     double *smem;
     double *partials;
@@ -167,6 +171,8 @@ struct Grid {
     unsigned long long epoch;
     GridSync gs;
 
+    __device__ __forceinline__ bool sync() { return grid_barrier(gs, epoch); }
+    __device__ __forceinline__ bool leader() const { return bid == 0 && threadIdx.x == 0; }
     // Consecutive grid reductions alternate between two partial regions: a
     // block may publish reduction j+1 while a slower block still reads
     // reduction j, but never reduction j+2 (a barrier separates them).
@@ -175,6 +181,34 @@ struct Grid {
         ++red;
         return p;
     }
+    template <int NV>
+    __device__ __forceinline__ bool allreduce(double (&v)[NV]) {
+        double *pr = part();
+        publish_partials<NV>(v, pr, smem);
+        if (!sync()) return false;
+        gather_partials<NV>(pr, v, smem);
+        return true;
+    }
+    template <int NV>
+    __device__ __forceinline__ bool allmax(double (&v)[NV]) {
+        double *pr = part();
+        publish_max<NV>(v, pr, smem);
+        if (!sync()) return false;
+        gather_max<NV>(pr, v, smem);
+        return true;
+    }
+};
+
+struct BlockTeam {
+    int r0, r1, gtid, gstride;
+    double *smem;
+
+    __device__ __forceinline__ bool sync() { __syncthreads(); return true; }
+    __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+    template <int NV>
+    __device__ __forceinline__ bool allreduce(double (&v)[NV]) { block_sum<NV>(v, smem); return true; }
+    template <int NV>
+    __device__ __forceinline__ bool allmax(double (&v)[NV]) { block_max<NV>(v, smem); return true; }
 };
 
 template <typename T>
@@ -243,9 +277,9 @@ struct alignas(4 * sizeof(T)) KRec {
     T p, v, r, c;
 };
 
-#define OHM_SYNC_OR(ret)                               \
-    do {                                               \
-        if (!grid_barrier(g.gs, g.epoch)) return ret;  \
+#define OHM_SYNC_OR(ret)                \
+    do {                                \
+        if (!g.sync()) return ret;      \
     } while (0)
 
 struct KrylovOut {
@@ -263,8 +297,8 @@ struct KrylovOut {
 // The early exit on ||s|| (bicgstab.rs:134-139) is taken after CD; t is then
 // simply unused.  Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On
 // success the correction is left in a.dx (FP64) for the rows of this block.
-template <typename T, int LPR>
-__device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
+template <typename T, int LPR, class Team>
+__device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                       int max_it, bool accept_partial, KrylovOut &out) {
     using Acc = T;   // FP32 SpMV accumulates in FP32, FP64 in FP64; dots always in FP64
     const int r0 = g.r0, r1 = g.r1;
@@ -309,10 +343,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
         acc0[0] += (double)rt * (double)rt;
     }
     {
-        double *pr = g.part();
-        publish_partials<1>(acc0, pr, g.smem);
-        OHM_SYNC_OR(kKrylovAbort);
-        gather_partials<1>(pr, acc0, g.smem);
+        if (!g.template allreduce<1>(acc0)) return kKrylovAbort;
     }
     const double r0norm = sqrt(acc0[0]);
     const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
@@ -384,10 +415,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
                 acc1[1] += (double)o.v * (double)o.v;
             });
             {
-                double *pr = g.part();
-                publish_partials<2>(acc1, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc1, g.smem);
+                if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
             }
             if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
@@ -424,10 +452,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
                 acc3[2] += (double)ti * (double)ti;
             });
             {
-                double *pr = g.part();
-                publish_partials<3>(acc3, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<3>(pr, acc3, g.smem);
+                if (!g.template allreduce<3>(acc3)) return kKrylovAbort;
             }
             if (sqrt(acc3[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
@@ -448,10 +473,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
                 acc4[1] += (double)rt * (double)rt;
             }
             {
-                double *pr = g.part();
-                publish_partials<2>(acc4, pr, g.smem);
-                OHM_SYNC_OR(kKrylovAbort);
-                gather_partials<2>(pr, acc4, g.smem);
+                if (!g.template allreduce<2>(acc4)) return kKrylovAbort;
             }
             { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
             rho_new = acc4[0];
@@ -482,28 +504,18 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Grid &g, double tol_f
 namespace ohm {
 
 // One Krylov solve of J d = r64 with the configured preconditioner.
-template <typename T, int LPR>
-__device__ __forceinline__ int krylov_any(const KernelArgs &a, Grid &g, double tol_floor, double inner_rtol,
+template <typename T, int LPR, class Team>
+__device__ __forceinline__ int krylov_any(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                           int max_it, bool accept_partial, KrylovOut &out) {
     if (a.precond == kPcIsai) return krylov_isai<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
     return krylov<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
 }
 
-template <int LPR>
-__global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
-    __shared__ double smem[32 * 4];
-    Grid g;
-    g.G = gridDim.x;
-    g.bid = blockIdx.x;
-    g.r0 = (int)(((long long)a.n * g.bid) / g.G);
-    g.r1 = (int)(((long long)a.n * (g.bid + 1)) / g.G);
-    g.gtid = g.bid * blockDim.x + threadIdx.x;
-    g.gstride = g.G * blockDim.x;
-    g.smem = smem;
-    g.partials = a.partials;
-    g.red = 0;
-    g.epoch = 0;
-    g.gs = a.gs;
+// The Newton loop (or a linear solve with refinement) for one system, run by
+// a team.  On return the leader thread has written `*info`; a false return
+// means a grid barrier gave up (nothing written).
+template <int LPR, class Team>
+__device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceInfo *info) {
     const int r0 = g.r0, r1 = g.r1, gtid = g.gtid, gstride = g.gstride;
 
     int status = kOk, kcode = kKrylovRunning, outer_done = 0, err_iter = 0;
@@ -531,7 +543,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
                                   a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)a.nq + 2 * (size_t)m);
                 }
             }
-            OHM_SYNC_OR();
+            OHM_SYNC_OR(false);
             // stamp map: each touched slot / row = base + contributions in canonical order
             for (int k = gtid; k < a.n_mslots + a.n_rrows; k += gstride) {
                 if (k < a.n_mslots) {
@@ -548,7 +560,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
                     a.b[row] = acc;
                 }
             }
-            OHM_SYNC_OR();
+            OHM_SYNC_OR(false);
         }
 
         // -------------------------- FP64 residual r64 = b - A x -------------------------
@@ -565,10 +577,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
             if (!isfinite(ri)) acc[2] += 1.0;
         });
         {
-            double *pr = g.part();
-            publish_partials<3>(acc, pr, g.smem);
-            OHM_SYNC_OR();
-            gather_partials<3>(pr, acc, g.smem);
+            if (!g.template allreduce<3>(acc)) return false;
         }
         const double bnorm = sqrt(acc[0]);
         const double rnorm64 = sqrt(acc[1]);
@@ -591,7 +600,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
         // ISAI(1) factorisation of the current matrix (once per outer iteration
         // of a Newton solve, once for a linear solve)
         if (a.precond == kPcIsai && (a.newton || outer == 0)) {
-            if (!isai_setup(a, g)) return;
+            if (!isai_setup(a, g)) return false;
         }
 
         // -------------------------------- BiCGSTAB ---------------------------------
@@ -616,24 +625,24 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
         int it32 = 0, it64 = 0;
         if (a.mixed) {
             kcode = krylov_any<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, a.max_krylov), true, ko);
-            if (kcode == kKrylovAbort) return;
+            if (kcode == kKrylovAbort) return false;
             it32 = ko.iterations;
             restarts += ko.restarts;
             if (kcode != kKrylovConverged) {
                 ++fallbacks;           // FP32 failed or stalled: redo this solve in FP64
                 kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
-                if (kcode == kKrylovAbort) return;
+                if (kcode == kKrylovAbort) return false;
                 it64 = ko.iterations;
                 restarts += ko.restarts;
             }
         } else {
             kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
-            if (kcode == kKrylovAbort) return;
+            if (kcode == kKrylovAbort) return false;
             it64 = ko.iterations;
             restarts += ko.restarts;
         }
         kiters += it32 + it64;
-        if (a.trace && outer < a.trace_cap && g.bid == 0 && threadIdx.x == 0) {
+        if (a.trace && outer < a.trace_cap && g.leader()) {
             double *tr = a.trace + (size_t)outer * kTraceCols;
             tr[0] = it32; tr[1] = it64; tr[2] = rnorm64; tr[3] = eta; tr[4] = -1.0; tr[5] = ko.restarts;
         }
@@ -647,7 +656,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
         // -------------------------------- update ----------------------------------
         if (!a.newton) {
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = a.x[i] + a.dx[i];
-            OHM_SYNC_OR();
+            OHM_SYNC_OR(false);
             outer_done = outer + 1;
             continue;      // next refinement sweep recomputes the FP64 residual
         }
@@ -657,7 +666,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
             a.x[i] = xo + a.dx[i];
             a.node_scale[i] = 0x3FF0000000000000ULL;   // 1.0
         }
-        OHM_SYNC_OR();
+        OHM_SYNC_OR(false);
         {
             const int ndev = a.nd + a.nq + a.nm;
             for (int k = gtid; k < ndev; k += gstride) {
@@ -666,7 +675,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
                 else mosfet_limit(a.mosfets[k - a.nd - a.nq], a.x_prev, a.x, a.node_scale);
             }
         }
-        OHM_SYNC_OR();
+        OHM_SYNC_OR(false);
         {
             double mx[3] = {0.0, 0.0, 0.0};   // max|dx|, max|x|, non-finite count
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
@@ -678,13 +687,10 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
                 mx[0] = fmax(mx[0], fabs(xn - xo));
                 mx[1] = fmax(mx[1], fabs(xn));
             }
-            double *pr = g.part();
-            publish_max<3>(mx, pr, g.smem);
-            OHM_SYNC_OR();
-            gather_max<3>(pr, mx, g.smem);
+            if (!g.template allmax<3>(mx)) return false;
             last_dmax = mx[0];
             outer_done = outer + 1;
-            if (a.trace && outer < a.trace_cap && g.bid == 0 && threadIdx.x == 0)
+            if (a.trace && outer < a.trace_cap && g.leader())
                 a.trace[(size_t)outer * kTraceCols + 4] = mx[0];
             if (mx[2] > 0.0) { status = kErrNewtonNumerical; err_iter = outer; break; }
             if (mx[0] < a.abs_tol + a.rel_tol * mx[1]) { status = kOk; break; }
@@ -702,10 +708,7 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
             const double ri = a.b[i] - ax;
             acc[0] += ri * ri;
         });
-        double *pr = g.part();
-        publish_partials<1>(acc, pr, g.smem);
-        OHM_SYNC_OR();
-        gather_partials<1>(pr, acc, g.smem);
+        if (!g.template allreduce<1>(acc)) return false;
         final_res = sqrt(acc[0]);
         if (a.require_true_residual && !(final_res < a.krylov_tol * bnorm_last)) {
             // refinement sweeps exhausted without reaching the FP64 tolerance
@@ -714,19 +717,40 @@ __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs 
         }
     }
 
-    if (g.bid == 0 && threadIdx.x == 0) {
-        a.info->status = status;
-        a.info->krylov_code = kcode;
-        a.info->iterations = outer_done;
-        a.info->error_iteration = err_iter;
-        a.info->krylov_iterations = kiters;
-        a.info->fp64_fallbacks = fallbacks;
-        a.info->krylov_restarts = restarts;
-        a.info->max_residual = last_dmax;
-        a.info->final_residual = final_res;
-        a.info->b_norm = bnorm_last;
+    if (g.leader()) {
+        info->status = status;
+        info->krylov_code = kcode;
+        info->iterations = outer_done;
+        info->error_iteration = err_iter;
+        info->krylov_iterations = kiters;
+        info->fp64_fallbacks = fallbacks;
+        info->krylov_restarts = restarts;
+        info->max_residual = last_dmax;
+        info->final_residual = final_res;
+        info->b_norm = bnorm_last;
     }
+    return true;
 }
+
+// One large system per launch: the whole (co-resident) grid is the team.
+template <int LPR>
+__global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
+    __shared__ double smem[32 * 4];
+    GridTeam g;
+    g.G = gridDim.x;
+    g.bid = blockIdx.x;
+    g.r0 = (int)(((long long)a.n * g.bid) / g.G);
+    g.r1 = (int)(((long long)a.n * (g.bid + 1)) / g.G);
+    g.gtid = g.bid * blockDim.x + threadIdx.x;
+    g.gstride = g.G * blockDim.x;
+    g.smem = smem;
+    g.partials = a.partials;
+    g.red = 0;
+    g.epoch = 0;
+    g.gs = a.gs;
+    solve_body<LPR>(a, g, a.info);
+}
+
 
 #undef OHM_SYNC_OR
 

@@ -332,6 +332,94 @@ class NewtonPlan:
         return xn
 
 
+class NewtonBatch:
+    """Many independent nonlinear systems (``MnaSystem`` each) packed into one
+    block-diagonal CSR and solved by one launch, one thread block per system.
+
+    The reference solves one circuit per ``newton_solve`` call
+    (src/solver/newton.rs:62-430); every instance here runs that loop.
+    ``row_off`` gives each instance's rows in the packed solution vector.
+    """
+
+    def __init__(self, systems, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        systems = list(systems)
+        if not systems:
+            raise InvalidArgument("empty batch")
+        self.n_instances = len(systems)
+        sizes = np.array([int(s.size) for s in systems], dtype=np.int64)
+        nnzs = np.array([int(s.g.nnz) for s in systems], dtype=np.int64)
+        self.row_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        self.nnz_off = np.concatenate([[0], np.cumsum(nnzs)]).astype(np.int64)
+        self.rows = int(self.row_off[-1])
+        rp = np.concatenate([np.asarray(s.g.row_ptr, dtype=np.uint32) for s in systems])
+        ci = np.concatenate([np.asarray(s.g.col, dtype=np.uint32) for s in systems])
+        vals = np.concatenate([np.asarray(s.g.val, dtype=np.float64) for s in systems])
+        bb = np.concatenate([np.asarray(s.b_dc, dtype=np.float64) for s in systems])
+
+        def pack(attr):
+            parts = [np.ascontiguousarray(getattr(s, attr)) for s in systems]
+            off = np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.int64)
+            return np.ascontiguousarray(np.concatenate(parts)), off
+
+        dd, doff = pack("diode_descriptors")
+        qd, qoff = pack("bjt_descriptors")
+        md, moff = pack("mosfet_descriptors")
+        vaf = None
+        if len(qd):
+            v = [np.full(len(s.bjt_descriptors), np.inf) if s.bjt_vaf is None else np.asarray(s.bjt_vaf, dtype=np.float64)
+                 for s in systems]
+            v = np.ascontiguousarray(np.concatenate(v))
+            if np.any(np.isfinite(v)):
+                vaf = v
+        rp = np.ascontiguousarray(rp)
+        ci = np.ascontiguousarray(ci)
+        h = C.c_void_p()
+        st = self.ctx.lib.ohm_batch_create(
+            self.ctx.handle, self.n_instances, vptr(self.row_off), vptr(self.nnz_off), u32ptr(rp), u32ptr(ci),
+            dptr(vals), dptr(bb), vptr(doff), vptr(dd), vptr(qoff), vptr(qd),
+            None if vaf is None else dptr(vaf), vptr(moff), vptr(md), C.byref(h))
+        if st != _lib.OK:
+            _raise(st)
+        self._h = h
+        self.last_info = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.ohm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def split(self, x):
+        """Per-instance views of a packed solution vector."""
+        return [x[self.row_off[i]:self.row_off[i + 1]] for i in range(self.n_instances)]
+
+    def newton_device(self, x_dev_ptr: int, params: NewtonParams | None = None, check: bool = True) -> dict:
+        """Newton on every instance over the packed device vector ``x_dev_ptr``
+        (``rows`` doubles, initial guess in, solution out)."""
+        p, keep = (params or NewtonParams()).to_c()
+        info = _lib.SolveInfo()
+        st = self.ctx.lib.ohm_batch_newton_device(self._h, C.c_void_p(int(x_dev_ptr)), C.byref(p),
+                                                  C.byref(info))
+        del keep
+        self.last_info = info.as_dict()
+        if st != _lib.OK and check:
+            _raise(st, info)
+        return self.last_info
+
+    def instance_info(self):
+        arr = (_lib.SolveInfo * self.n_instances)()
+        st = self.ctx.lib.ohm_batch_instance_info(self._h, arr, self.n_instances)
+        if st:
+            _raise(st)
+        return [a.as_dict() for a in arr]
+
+
 class DeviceBuffer:
     """``SolverBackend::Buffer``: FP64 device vector."""
 

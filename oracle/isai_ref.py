@@ -15,6 +15,12 @@ Device variant (numpy, exact sequential ILU(0)):
   ILU(0) on A's pattern plus the diagonal, no pivoting; ISAI(1) columns on the
   level-1 patterns as triangular solves.  The device computes the same factor
   approximately (Chow-Patel sweeps).
+
+Device variant, step by step (``chow_patel_ref``, ``isai1_device_ref``):
+  the factor after a fixed number of Jacobi-style Chow-Patel sweeps
+  (E. Chow, A. Patel, "Fine-grained parallel incomplete LU factorization",
+  SIAM J. Sci. Comput. 37(2), 2015), then ISAI(1) columns capped at 32 rows
+  nearest the diagonal; the device result agrees to rounding.
 """
 from __future__ import annotations
 
@@ -168,3 +174,87 @@ def ilu0_augmented(n, row_ptr, col, val):
     L = np.tril(W, -1) * P + np.eye(n)
     U = np.triu(W) * P
     return L, U
+
+
+def _augmented_pattern(n, row_ptr, col):
+    P = np.zeros((n, n), dtype=bool)
+    for i in range(n):
+        for k in range(row_ptr[i], row_ptr[i + 1]):
+            P[i, col[k]] = True
+        P[i, i] = True
+    return P
+
+
+def chow_patel_ref(n, row_ptr, col, val, sweeps=6):
+    """ILU(0) factor on the augmented pattern after ``sweeps`` Jacobi-style
+    fixed-point sweeps.  Start: U = upper(A), L_ij = A_ij / A_jj (A_jj = 0
+    leaves A_ij).  Sweep, every pattern entry from the previous iterate:
+    l_ij = (a_ij - sum_{k<j} l_ik u_kj) / u_jj (j < i; u_jj = 0 leaves the
+    numerator), u_ij = a_ij - sum_{k<i} l_ik u_kj (j >= i).  Returns dense L
+    (unit diagonal) and U."""
+    A = np.zeros((n, n))
+    for i in range(n):
+        for k in range(row_ptr[i], row_ptr[i + 1]):
+            A[i, col[k]] = val[k]
+    P = _augmented_pattern(n, row_ptr, col)
+    Lo = np.zeros((n, n))
+    Up = np.zeros((n, n))
+    d = np.diag(A)
+    for i in range(n):
+        for j in np.nonzero(P[i])[0]:
+            if j < i:
+                Lo[i, j] = A[i, j] / d[j] if abs(d[j]) > 1e-300 else A[i, j]
+            else:
+                Up[i, j] = A[i, j]
+    for _ in range(sweeps):
+        Ln = np.zeros_like(Lo)
+        Un = np.zeros_like(Up)
+        for i in range(n):
+            for j in np.nonzero(P[i])[0]:
+                m = min(i, j)
+                acc = A[i, j]
+                for k in np.nonzero(P[i, :m])[0]:
+                    if P[k, j]:
+                        acc -= Lo[i, k] * Up[k, j]
+                if j < i:
+                    ujj = Up[j, j]
+                    Ln[i, j] = acc / ujj if abs(ujj) > 1e-300 else acc
+                else:
+                    Un[i, j] = acc
+        Lo, Up = Ln, Un
+    return Lo + np.eye(n), Up, P
+
+
+def isai1_device_ref(n, row_ptr, col, val, sweeps=6, cap=32):
+    """ISAI(1) of the Chow-Patel factor: pattern(M_L) = pattern((L+I)^2),
+    pattern(M_U) = pattern(U^2) over the augmented pattern; column k solves the
+    local triangular system on its rows J (at most ``cap``: the smallest rows
+    for M_L, the largest for M_U); a zero U pivot gives a zero entry.
+    Returns dense M_L, M_U."""
+    L, U, P = chow_patel_ref(n, row_ptr, col, val, sweeps)
+    PL = np.tril(P)
+    PU = np.triu(P)
+    pat_l = (PL.astype(np.int64) @ PL.astype(np.int64)) > 0
+    pat_u = (PU.astype(np.int64) @ PU.astype(np.int64)) > 0
+    ML = np.zeros((n, n))
+    MU = np.zeros((n, n))
+    for k in range(n):
+        J = np.nonzero(pat_l[:, k])[0][:cap]
+        m = np.zeros(len(J))
+        for x, rx in enumerate(J):
+            acc = 1.0 if rx == k else 0.0
+            for y in range(x):
+                acc -= L[rx, J[y]] * m[y]
+            m[x] = acc
+        ML[J, k] = m
+        J = np.nonzero(pat_u[:, k])[0]
+        J = J[max(0, len(J) - cap):]
+        m = np.zeros(len(J))
+        for x in range(len(J) - 1, -1, -1):
+            rx = J[x]
+            acc = 1.0 if rx == k else 0.0
+            for y in range(x + 1, len(J)):
+                acc -= U[rx, J[y]] * m[y]
+            m[x] = acc / U[rx, rx] if abs(U[rx, rx]) > 1e-300 else 0.0
+        MU[J, k] = m
+    return ML, MU

@@ -6,6 +6,7 @@ import pytest
 
 from oracle import devices_ref, linear_ref, mna_ref
 from oracle.mna_ref import RefCsr
+from ohmnivore_b200 import circuits as ck
 from ohmnivore_b200 import mna
 from tests.golden import known_answers as KA
 
@@ -308,3 +309,23 @@ def test_ilu0_augmented_matches_lu_on_tridiagonal():
     rp, ci, v = _ref_csr(3, trip)
     L, U = isai_ref.ilu0_augmented(3, rp, ci, v)
     assert abs(U[2, 2] - (-1.0 / (g1 + g2))) < 1e-9
+
+
+def test_chow_patel_converges_to_ilu0():
+    """Enough Chow-Patel sweeps reach the exact ILU(0) factor of the augmented
+    pattern (the fixed point), on a small MNA mesh with a source branch row."""
+    s = mna.compile_circuit(ck.diode_mesh(4, 4, seed=2, diode_frac=0.0))
+    L, U, _ = isai_ref.chow_patel_ref(s.size, s.g.row_ptr, s.g.col, s.g.val, sweeps=2 * s.size)
+    Le, Ue = isai_ref.ilu0_augmented(s.size, s.g.row_ptr, s.g.col, s.g.val)
+    np.testing.assert_allclose(L, Le, atol=1e-12 * np.abs(Le).max())
+    np.testing.assert_allclose(U, Ue, atol=1e-12 * np.abs(Ue).max())
+
+
+def test_isai1_device_variant_exact_when_pattern_is_full():
+    """With no fill beyond L^2 (a tridiagonal of size 3) and converged sweeps,
+    M_L = L^-1 and M_U = U^-1."""
+    rp, ci, v = _ref_csr(3, _TRI3)
+    ML, MU = isai_ref.isai1_device_ref(3, rp, ci, v, sweeps=8)
+    L, U, _ = isai_ref.chow_patel_ref(3, rp, ci, v, sweeps=8)
+    np.testing.assert_allclose(ML @ L, np.eye(3), atol=1e-12)
+    np.testing.assert_allclose(MU @ U, np.eye(3), atol=1e-12)
