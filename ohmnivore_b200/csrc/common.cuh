@@ -131,24 +131,23 @@ __device__ __forceinline__ void publish_partials(double (&v)[NV], double *partia
     }
 }
 
-// Grid reduction, step 2 (after a barrier): warp 0 of every block sums all
-// partials in the same fixed order (lane-strided, then a fixed shuffle tree)
-// and broadcasts through shared memory, so every block holds bit-identical
-// results.
+// Grid reduction, step 2 (after a barrier): in every block, warp k sums the
+// partials of value k in a fixed order (lane-strided, then a fixed shuffle
+// tree) and broadcasts through shared memory, so every block holds
+// bit-identical results; the NV values are gathered concurrently.
 template <int NV>
 __device__ __forceinline__ void gather_partials(const double *partials, double (&out)[NV],
                                                 double *smem) {
     const int G = gridDim.x;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < NV) {
+        const double *p = partials + (size_t)warp * G;
+        double s = 0.0;
+#pragma unroll 4
+        for (int j = lane; j < G; j += 32) s += __ldcg(p + j);
 #pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double s = 0.0;
-            for (int j = lane; j < G; j += 32) s += __ldcg(&partials[k * G + j]);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) smem[k] = s;
-        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) smem[warp] = s;
     }
     __syncthreads();
 #pragma unroll
@@ -169,16 +168,15 @@ template <int NV>
 __device__ __forceinline__ void gather_max(const double *partials, double (&out)[NV],
                                            double *smem) {
     const int G = gridDim.x;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < NV) {
+        const double *p = partials + (size_t)warp * G;
+        double s = 0.0;
+#pragma unroll 4
+        for (int j = lane; j < G; j += 32) s = fmax(s, __ldcg(p + j));
 #pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double s = 0.0;
-            for (int j = lane; j < G; j += 32) s = fmax(s, __ldcg(&partials[k * G + j]));
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
-            if (lane == 0) smem[k] = s;
-        }
+        for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+        if (lane == 0) smem[warp] = s;
     }
     __syncthreads();
 #pragma unroll

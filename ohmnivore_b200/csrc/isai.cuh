@@ -113,16 +113,27 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Team &g, double 
     out.iterations = 0;
     out.restarts = 0;
 
-    double acc0[1] = {0.0};
+    // stopping norm: scaled residual W r for Newton solves, as in krylov()
+    const bool wt = a.newton != 0;
+    double *w = a.dx;
+    double acc0[2] = {0.0, 0.0};
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         const T rt = cvt<T>(a.r64[i]);
         r[i] = rt; rhat[i] = rt; pin[i] = T(0); v[i] = T(0); d[i] = T(0);
+        double wi = 1.0;
+        if (wt) {
+            const uint32_t ds = a.diag_slot[i];
+            const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
+            if (fabs(aii) > 1e-30) wi = 1.0 / fabs(aii);
+            w[i] = wi;
+        }
         acc0[0] += (double)rt * (double)rt;
+        acc0[1] += (wi * (double)rt) * (wi * (double)rt);
     }
     {
-        if (!g.template allreduce<1>(acc0)) return kKrylovAbort;
+        if (!g.template allreduce<2>(acc0)) return kKrylovAbort;
     }
-    const double r0norm = sqrt(acc0[0]);
+    const double r0norm = sqrt(acc0[1]);
     const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
     double rr_cur = acc0[0], rhat2 = acc0[0], rho_new = acc0[0];
     double rho = 1.0, alpha = 1.0, omega = 1.0;
@@ -198,7 +209,8 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Team &g, double 
                                        const T si = s_of(i, false);
                                        s[i] = si;
                                        y[i] = cvt<T>(yy);
-                                       acc2[0] += (double)si * (double)si;
+                                       const double ws = wt ? w[i] * (double)si : (double)si;
+                                       acc2[0] += ws * ws;
                                    });
             {
                 if (!g.template allreduce<1>(acc2)) return kKrylovAbort;
@@ -228,20 +240,22 @@ __device__ __forceinline__ int krylov_isai(const KernelArgs &a, Team &g, double 
             }
             if (!(acc3[1] > 0.0)) { code = kKrylovBreakTt; break; }
             omega = acc3[0] / acc3[1];
-            double acc4[2] = {0.0, 0.0};
+            double acc4[3] = {0.0, 0.0, 0.0};
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                 d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omega * (double)shat[i]);
                 const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
                 r[i] = rt;
+                const double wr = wt ? w[i] * (double)rt : (double)rt;
                 acc4[0] += (double)rhat[i] * (double)rt;
                 acc4[1] += (double)rt * (double)rt;
+                acc4[2] += wr * wr;
             }
             {
-                if (!g.template allreduce<2>(acc4)) return kKrylovAbort;
+                if (!g.template allreduce<3>(acc4)) return kKrylovAbort;
             }
             rho_new = acc4[0];
             rr_cur = acc4[1];
-            const double rnorm = sqrt(acc4[1]);
+            const double rnorm = sqrt(acc4[2]);
             if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
             if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
             if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }

@@ -297,6 +297,12 @@ struct KrylovOut {
 // The early exit on ||s|| (bicgstab.rs:134-139) is taken after CD; t is then
 // simply unused.  Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On
 // success the correction is left in a.dx (FP64) for the rows of this block.
+//
+// Newton solves measure that stopping norm on the diagonally scaled residual
+// W r, w_i = 1/|J_ii| (1 for a zero diagonal): volts instead of amperes, so a
+// junction row with a huge conductance cannot hide unresolved corrections on
+// the other rows behind a relative tolerance.  a.dx holds w during the solve.
+// Linear solves keep the reference's unscaled ||r|| < tol ||b||.
 template <typename T, int LPR, class Team>
 __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                       int max_it, bool accept_partial, KrylovOut &out) {
@@ -312,13 +318,17 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
     out.restarts = 0;
 
     // ---- start: r = r64, r_hat = r, p = v = d = 0; preconditioner coefficients ----
-    double acc0[1] = {0.0};
+    const bool wt = a.newton != 0;
+    double *w = a.dx;
+    double acc0[2] = {0.0, 0.0};     // ||r||^2, ||W r||^2
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         const T rt = cvt<T>(a.r64[i]);
         double cs = 0.0, cp = 0.0;
+        const uint32_t ds = a.diag_slot[i];
+        const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
+        const double wi = (wt && fabs(aii) > 1e-30) ? 1.0 / fabs(aii) : 1.0;
+        if (wt) w[i] = wi;
         if (a.precond != kPcNone) {
-            const uint32_t ds = a.diag_slot[i];
-            const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
             const int pi = partner[i];
             if (a.precond == kPcAuto && pi >= 0) {
                 const double akk = a.diag_slot[pi] == kSentinel ? 0.0 : a.vals64[a.diag_slot[pi]];
@@ -341,11 +351,12 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
         rhat[i] = rt;
         d[i] = T(0);
         acc0[0] += (double)rt * (double)rt;
+        acc0[1] += (wi * (double)rt) * (wi * (double)rt);
     }
     {
-        if (!g.template allreduce<1>(acc0)) return kKrylovAbort;
+        if (!g.template allreduce<2>(acc0)) return kKrylovAbort;
     }
-    const double r0norm = sqrt(acc0[0]);
+    const double r0norm = sqrt(acc0[1]);            // stopping norm (scaled for Newton)
     const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
     double rr_cur = acc0[0];          // ||r||^2
     double rhat2 = acc0[0];           // ||r_hat||^2
@@ -440,21 +451,23 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 }
                 return cvt<T>(z);
             };
-            double acc3[3] = {0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t)
+            double acc3[4] = {0.0, 0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t), ||W s||^2
             spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, shat_at, [&](int i, double y) {
                 const T si = s_of(nxt[i]);
                 const T ti = cvt<T>(y);
                 s[i] = si;
                 t[i] = ti;
                 shat[i] = shat_at(i, true);
+                const double ws = wt ? w[i] * (double)si : (double)si;
                 acc3[0] += (double)si * (double)si;
                 acc3[1] += (double)ti * (double)si;
                 acc3[2] += (double)ti * (double)ti;
+                acc3[3] += ws * ws;
             });
             {
-                if (!g.template allreduce<3>(acc3)) return kKrylovAbort;
+                if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
             }
-            if (sqrt(acc3[0]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
+            if (sqrt(acc3[3]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
                     d[i] = cvt<T>((double)d[i] + al * (double)phat[i]);
                 code = kKrylovConverged;
@@ -464,21 +477,23 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             if (!(acc3[2] > 0.0)) { code = kKrylovBreakTt; break; }
             omega = acc3[1] / acc3[2];
             // ---------------- E: d, r updates ----------------
-            double acc4[2] = {0.0, 0.0};
+            double acc4[3] = {0.0, 0.0, 0.0};   // (r_hat, r), ||r||^2, ||W r||^2
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                 d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omega * (double)shat[i]);
                 const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
                 nxt[i].r = rt;
+                const double wr = wt ? w[i] * (double)rt : (double)rt;
                 acc4[0] += (double)rhat[i] * (double)rt;
                 acc4[1] += (double)rt * (double)rt;
+                acc4[2] += wr * wr;
             }
             {
-                if (!g.template allreduce<2>(acc4)) return kKrylovAbort;
+                if (!g.template allreduce<3>(acc4)) return kKrylovAbort;
             }
             { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
             rho_new = acc4[0];
             rr_cur = acc4[1];
-            const double rnorm = sqrt(acc4[1]);
+            const double rnorm = sqrt(acc4[2]);
             if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
             if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
             if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }
@@ -564,7 +579,10 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
         }
 
         // -------------------------- FP64 residual r64 = b - A x -------------------------
-        double acc[3] = {0.0, 0.0, 0.0};   // ||b||^2, ||r||^2, #non-finite
+        // ||b||^2, ||r||^2, and for Newton the scaled ||W b||^2, ||W r||^2
+        // (w_i = 1/|J_ii|, the stopping scale of krylov()).  A non-finite
+        // entry makes ||r||^2 non-finite.
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         const double *xv = a.x;
         auto x_at = [&](int j, bool) -> double { return xv[j]; };
         spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at,
@@ -574,15 +592,23 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
             a.r64[i] = ri;
             acc[0] += bi * bi;
             acc[1] += ri * ri;
-            if (!isfinite(ri)) acc[2] += 1.0;
+            if (a.newton) {
+                const uint32_t ds = a.diag_slot[i];
+                const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
+                const double wi = fabs(aii) > 1e-30 ? 1.0 / fabs(aii) : 1.0;
+                acc[2] += (wi * bi) * (wi * bi);
+                acc[3] += (wi * ri) * (wi * ri);
+            }
         });
         {
-            if (!g.template allreduce<3>(acc)) return false;
+            if (!g.template allreduce<4>(acc)) return false;
         }
         const double bnorm = sqrt(acc[0]);
+        const double bnorm_w = a.newton ? sqrt(acc[2]) : bnorm;   // Krylov stopping scale
+        const double fnorm_w = a.newton ? sqrt(acc[3]) : sqrt(acc[1]);
         const double rnorm64 = sqrt(acc[1]);
         bnorm_last = bnorm;
-        if (a.newton && acc[2] > 0.0) {
+        if (a.newton && !isfinite(acc[1])) {
             // non-finite assembled system (newton.rs:258-263)
             status = kErrNewtonNumerical;
             err_iter = outer;
@@ -604,13 +630,13 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
         }
 
         // -------------------------------- BiCGSTAB ---------------------------------
-        const double floor_tol = a.krylov_tol * bnorm;
+        const double floor_tol = a.krylov_tol * bnorm_w;
         // Inner tolerance: constant, or Eisenstat-Walker choice 2 (gamma 0.9,
-        // exponent 2, safeguarded) on the Newton residual ||b - J x||.
+        // exponent 2, safeguarded) on the scaled Newton residual ||W (b - J x)||.
         double eta = a.inner_rtol;
         if (a.newton && a.forcing == 1) {
             if (fnorm_prev > 0.0) {
-                const double ratio = rnorm64 / fnorm_prev;
+                const double ratio = fnorm_w / fnorm_prev;
                 eta = 0.9 * ratio * ratio;
                 const double guard = 0.9 * eta_prev * eta_prev;
                 if (guard > 0.1) eta = fmax(eta, guard);
@@ -619,7 +645,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
             }
             eta = fmin(fmax(eta, a.inner_rtol), a.eta_max);
             eta_prev = eta;
-            fnorm_prev = rnorm64;
+            fnorm_prev = fnorm_w;
         }
         KrylovOut ko{0, 0};
         int it32 = 0, it64 = 0;
