@@ -117,6 +117,11 @@ typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + 
     const double *initial_guess; /* NewtonParams::initial_guess, host pointer, may be NULL */
     int32_t forcing;             /* ohm_forcing, default constant */
     double eta_max;              /* Eisenstat-Walker upper bound, default 0.5 */
+    int32_t continuation;        /* 1: when the direct solve fails, run the reference's DC strategy on
+                                    the device (src/analysis/dc.rs:60-290): source stepping (MOSFET
+                                    circuits), GMIN stepping, pseudo-transient continuation; default 0 */
+    int32_t n_nodes;             /* node rows (the first rows of the MNA system); required with
+                                    continuation, which adds GMIN to their diagonals */
 } ohm_newton_params;
 
 typedef struct {
@@ -131,6 +136,8 @@ typedef struct {
     double final_residual_norm;  /* ||b - A x||_2 at exit (FP64), when computed */
     double b_norm;               /* ||b||_2 of the last linear system */
     int64_t kernel_launches;     /* kernels this call launched */
+    int32_t continuation_steps;  /* Newton runs of the DC continuation after the direct attempt */
+    int32_t continuation_kind;   /* last continuation stage: 0 none, 1 source, 2 GMIN, 3 pseudo-transient */
 } ohm_solve_info;
 
 /* Reference defaults; fill before changing fields. */
@@ -264,14 +271,16 @@ ohm_status ohm_plan_limit(ohm_plan *plan, const double *x_old_host, double *x_ne
  *              indices in their descriptors.
  * base_b and the solution vector are packed by rows.  Each instance is solved
  * by one thread block with the block-Jacobi preconditioner (ISAI(1) is
- * rejected), largest instances first. */
+ * rejected), largest instances first.  n_nodes (per instance, may be NULL)
+ * enables params->continuation; params->n_nodes is ignored for batches. */
 typedef struct ohm_batch ohm_batch;
 ohm_status ohm_batch_create(ohm_ctx *ctx, int64_t n_instances, const int64_t *row_off, const int64_t *nnz_off,
                             const uint32_t *row_ptrs, const uint32_t *col_indices,
                             const double *base_g_values, const double *base_b,
                             const int64_t *diode_off, const ohm_diode_desc *diodes,
                             const int64_t *bjt_off, const ohm_bjt_desc *bjts, const double *bjt_vaf,
-                            const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets, ohm_batch **out);
+                            const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets,
+                            const int32_t *n_nodes, ohm_batch **out);
 ohm_status ohm_batch_destroy(ohm_batch *batch);
 /* Newton on every instance.  x_inout_device: row_off[n] doubles.  `summary`
  * gets totals (iterations = the largest Newton count, error_iteration = the

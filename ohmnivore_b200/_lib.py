@@ -30,7 +30,8 @@ class KrylovParams(C.Structure):
 class NewtonParamsC(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
                 ("krylov", KrylovParams), ("initial_guess", C.POINTER(C.c_double)),
-                ("forcing", C.c_int32), ("eta_max", C.c_double)]
+                ("forcing", C.c_int32), ("eta_max", C.c_double), ("continuation", C.c_int32),
+                ("n_nodes", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -38,7 +39,8 @@ class SolveInfo(C.Structure):
                 ("error_iteration", C.c_int32), ("krylov_iterations", C.c_int64),
                 ("fp64_fallbacks", C.c_int32), ("krylov_restarts", C.c_int32),
                 ("max_residual", C.c_double), ("final_residual_norm", C.c_double),
-                ("b_norm", C.c_double), ("kernel_launches", C.c_int64)]
+                ("b_norm", C.c_double), ("kernel_launches", C.c_int64),
+                ("continuation_steps", C.c_int32), ("continuation_kind", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -90,7 +92,7 @@ SIGNATURES = {
     "ohm_plan_limit": (C.c_int, [_vp, _dp, _dp]),
     "ohm_plan_trace": (C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int32)]),
     "ohm_batch_create": (C.c_int, [_vp, _i64, _vp, _vp, _u32p, _u32p, _dp, _dp, _vp, _vp, _vp, _vp, _dp,
-                                   _vp, _vp, C.POINTER(_vp)]),
+                                   _vp, _vp, _vp, C.POINTER(_vp)]),
     "ohm_batch_destroy": (C.c_int, [_vp]),
     "ohm_isai_apply": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64]),
     "ohm_batch_newton_device": (C.c_int, [_vp, _vp, C.POINTER(NewtonParamsC), C.POINTER(SolveInfo)]),

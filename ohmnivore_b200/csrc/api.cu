@@ -62,6 +62,8 @@ extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
     p->initial_guess = nullptr;
     p->forcing = OHM_FORCING_CONSTANT;
     p->eta_max = 0.5;
+    p->continuation = 0;
+    p->n_nodes = 0;
 }
 
 // ---------------------------------------------------------------- context --
@@ -236,6 +238,8 @@ ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, in
         info->final_residual_norm = di.final_residual;
         info->b_norm = di.b_norm;
         info->kernel_launches = launches;
+        info->continuation_steps = di.continuation_steps;
+        info->continuation_kind = di.continuation_kind;
     }
     return st;
 }
@@ -489,6 +493,8 @@ struct ohm_plan {
     uint32_t *mslot = nullptr, *mslot_ptr = nullptr, *mslot_ids = nullptr;
     uint32_t *rrow = nullptr, *rrow_ptr = nullptr, *rrow_ids = nullptr;
     unsigned long long *node_scale = nullptr;
+    uint8_t *stampflag = nullptr;      // per row: diagonal / rhs written by the stamp map
+    double *x_good = nullptr;          // DC continuation: last converged point
     double *trace = nullptr;           // kTraceRows x kTraceCols
     Workspace ws;
     IsaiDev isai;                      // built on the first ISAI(1) solve
@@ -508,6 +514,7 @@ static void plan_free(ohm_plan *p) {
     cudaFree(p->mslot); cudaFree(p->mslot_ptr); cudaFree(p->mslot_ids);
     cudaFree(p->rrow); cudaFree(p->rrow_ptr); cudaFree(p->rrow_ids);
     cudaFree(p->node_scale);
+    cudaFree(p->stampflag); cudaFree(p->x_good);
     cudaFree(p->trace);
     p->ws.release();
     p->isai.release();
@@ -563,6 +570,7 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     p->n_rrows = (int)rs.size();
     p->touched.assign(nnz, 0);
     for (uint32_t sl : ms) p->touched[sl] = 1;
+    std::vector<uint8_t> sflag = stamp_flags(size, row_ptrs, col_indices, p->touched, rs);
     p->h_rp.assign(row_ptrs, row_ptrs + size + 1);
     p->h_col.assign(col_indices, col_indices + nnz);
     build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, true, p->pc_pairs);
@@ -590,6 +598,8 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     if (e == cudaSuccess) e = up(&p->rrow_ptr, rptr.data(), rptr.size(), s);
     if (e == cudaSuccess) e = up(&p->rrow_ids, rids.data(), rids.size(), s);
     if (e == cudaSuccess) e = dalloc(&p->node_scale, size);
+    if (e == cudaSuccess) e = up(&p->stampflag, sflag.data(), size, s);
+    if (e == cudaSuccess) e = dalloc(&p->x_good, size);
     if (e == cudaSuccess) e = dalloc(&p->trace, (size_t)kTraceRows * kTraceCols);
     if (e == cudaSuccess) e = p->ws.alloc(size, c->num_sms);
     if (e == cudaSuccess && nnz) {
@@ -693,6 +703,10 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
     a.trace = p->trace;
     a.trace_cap = kTraceRows;
+    a.continuation = np->continuation ? 1 : 0;
+    a.n_nodes = (int)std::min<int64_t>(np->n_nodes, p->n);
+    a.stampflag = p->stampflag;
+    a.x_good = p->x_good;
     return OHM_OK;
 }
 
@@ -701,6 +715,8 @@ static ohm_status check_newton(const ohm_newton_params *np) {
     if (np->max_iterations <= 0)
         return fail(OHM_ERR_NEWTON_NOT_CONVERGED, "Newton solver did not converge after 0 iterations");
     if (!(np->abs_tol >= 0.0) || !(np->rel_tol >= 0.0)) return fail(OHM_ERR_INVALID_ARG, "negative tolerance");
+    if (np->continuation && np->n_nodes <= 0)
+        return fail(OHM_ERR_INVALID_ARG, "continuation needs n_nodes (the node rows of the MNA system)");
     return ohm_check_krylov(&np->krylov);
 }
 

@@ -29,6 +29,9 @@ struct BatchArgs {
     unsigned int *queue;            // next position in `order`
     DeviceInfo *infos;              // per instance
     double *node_scale_base;        // per row (8 bytes)
+    const int32_t *n_nodes;         // per instance (continuation), may be null
+    const uint8_t *stampflag;       // per row
+    double *x_good;                 // per row
 };
 
 template <typename P>
@@ -93,6 +96,9 @@ __global__ void __launch_bounds__(kBatchBlock) batch_solver(BatchArgs B) {
         a.rrow_ids = B.base.rrow_ids + B.rid_off[i];
         a.node_scale = (unsigned long long *)(B.node_scale_base + ro);
         a.trace = nullptr;
+        a.n_nodes = B.n_nodes ? B.n_nodes[i] : 0;
+        a.stampflag = B.stampflag + ro;
+        a.x_good = B.x_good + ro;
         BlockTeam g;
         g.r0 = 0;
         g.r1 = a.n;
@@ -149,7 +155,8 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
                                        const double *base_g_values, const double *base_b,
                                        const int64_t *diode_off, const ohm_diode_desc *diodes,
                                        const int64_t *bjt_off, const ohm_bjt_desc *bjts, const double *bjt_vaf,
-                                       const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets, ohm_batch **out) {
+                                       const int64_t *mosfet_off, const ohm_mosfet_desc *mosfets,
+                                       const int32_t *n_nodes, ohm_batch **out) {
     if (!c || !out || n_inst <= 0 || !row_off || !nnz_off || !row_ptrs || !base_g_values || !base_b ||
         !diode_off || !bjt_off || !mosfet_off)
         return ohm_fail(OHM_ERR_INVALID_ARG, "bad batch arguments");
@@ -168,7 +175,7 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     std::vector<uint32_t> mslot, mptr, mids, rrow, rptr, rids;
     std::vector<int32_t> partner(rows);
     std::vector<uint32_t> diag(rows), off(rows);
-    std::vector<uint8_t> flag(rows);
+    std::vector<uint8_t> flag(rows), sflag(rows);
     bool any_pair = false;
     int64_t max_nnz_row = 0;
     for (int64_t i = 0; i < n_inst; ++i) {
@@ -215,6 +222,10 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
         rids.insert(rids.end(), i2.begin(), i2.end());
         std::vector<char> touched(z, 0);
         for (uint32_t sl : s1) touched[sl] = 1;
+        if (n_nodes && (n_nodes[i] < 0 || n_nodes[i] > n))
+            return ohm_fail(OHM_ERR_INVALID_ARG, "instance %lld: n_nodes out of range", (long long)i);
+        const std::vector<uint8_t> sf = stamp_flags(n, rp, cl, touched, s2);
+        std::copy(sf.begin(), sf.end(), sflag.begin() + row_off[i]);
         PcHost pc;
         build_precond(n, rp, cl, base_g_values + nnz_off[i], touched, true, pc);
         std::copy(pc.partner.begin(), pc.partner.end(), partner.begin() + row_off[i]);
@@ -254,6 +265,9 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     ZERO(f64, rows); a.r64 = f64;
     ZERO(f64, rows); a.dx = f64;
     ZERO(f64, rows); b->args.node_scale_base = f64;
+    ZERO(f64, rows); b->args.x_good = f64;
+    { uint8_t *sf = nullptr; PUT(sf, sflag.data(), rows); b->args.stampflag = sf; }
+    if (n_nodes) { int32_t *nn = nullptr; PUT(nn, n_nodes, n_inst); b->args.n_nodes = nn; }
     int32_t *i32 = nullptr;
     PUT(i32, partner.data(), rows); a.partner = i32;
     PUT(u32, diag.data(), rows); a.diag_slot = u32;
@@ -326,6 +340,8 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
     if (st != OHM_OK) return st;
     if (np->krylov.precond == OHM_PRECOND_ISAI1)
         return ohm_fail(OHM_ERR_INVALID_ARG, "batched solves use block Jacobi (ISAI(1) is for single systems)");
+    if (np->continuation && !b->args.n_nodes)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "continuation needs the per-instance n_nodes given at creation");
     ohm_ctx *c = b->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
     BatchArgs B = b->args;
@@ -348,6 +364,7 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
     a.fp32_max_iterations = np->krylov.fp32_max_iterations > 0 ? np->krylov.fp32_max_iterations
                                                                : np->krylov.max_iterations;
     a.max_restarts = std::max(0, np->krylov.max_restarts);
+    a.continuation = np->continuation ? 1 : 0;
     if (np->initial_guess)
         CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, b->rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), c->stream));
@@ -363,13 +380,15 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
                              c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     // summary: worst status, totals
-    int64_t kit = 0, fb = 0, rs = 0, worst = -1;
-    int max_newton = 0;
+    int64_t kit = 0, fb = 0, rs = 0, worst = -1, csteps = 0;
+    int max_newton = 0, ckind = 0;
     for (int64_t i = 0; i < b->n_inst; ++i) {
         const DeviceInfo &d = b->host_infos[i];
         kit += d.krylov_iterations;
         fb += d.fp64_fallbacks;
         rs += d.krylov_restarts;
+        csteps += d.continuation_steps;
+        ckind = std::max(ckind, d.continuation_kind);
         max_newton = std::max(max_newton, d.iterations);
         if (d.status != 0 && worst < 0) worst = i;
     }
@@ -382,6 +401,8 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
         summary->kernel_launches = 1;
         summary->status = worst < 0 ? OHM_OK : b->host_infos[worst].status;
         summary->error_iteration = (int32_t)worst;
+        summary->continuation_steps = (int32_t)std::min<int64_t>(csteps, 0x7fffffff);
+        summary->continuation_kind = ckind;
     }
     if (worst >= 0) {
         const DeviceInfo &d = b->host_infos[worst];
@@ -408,6 +429,8 @@ extern "C" ohm_status ohm_batch_instance_info(ohm_batch *b, ohm_solve_info *info
         o.max_residual = d.max_residual;
         o.b_norm = d.b_norm;
         o.kernel_launches = 1;
+        o.continuation_steps = d.continuation_steps;
+        o.continuation_kind = d.continuation_kind;
     }
     return OHM_OK;
 }

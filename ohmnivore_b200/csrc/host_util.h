@@ -146,4 +146,16 @@ inline void build_stamp_map(const std::vector<std::pair<uint32_t, uint32_t>> &pa
 }
 
 
+// Per-row flags for the DC continuation: bit 0 = the row's diagonal slot is
+// written by the stamp map (touched_slot), bit 1 = its rhs entry is (rrows).
+inline std::vector<uint8_t> stamp_flags(int64_t n, const uint32_t *rp, const uint32_t *col,
+                                        const std::vector<char> &touched_slot, const std::vector<uint32_t> &rrows) {
+    std::vector<uint8_t> f(n, 0);
+    for (int64_t i = 0; i < n; ++i)
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if ((int64_t)col[k] == i && touched_slot[k]) f[i] |= 1;
+    for (uint32_t r : rrows) f[r] |= 2;
+    return f;
+}
+
 }  // namespace ohm

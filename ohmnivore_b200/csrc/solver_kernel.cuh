@@ -78,7 +78,12 @@ struct DeviceInfo {
     double max_residual;     // last max|x - x_old|
     double final_residual;   // ||b - A x||_2 (FP64) at exit, linear mode
     double b_norm;
+    int continuation_steps;  // Newton runs of the DC continuation after the direct attempt
+    int continuation_kind;   // kContNone / kContSource / kContGmin / kContPseudo: last stage used
 };
+
+// DC continuation stages (src/analysis/dc.rs:60-290).
+enum ContKind : int { kContNone = 0, kContSource = 1, kContGmin = 2, kContPseudo = 3 };
 
 struct KernelArgs {
     // CSR system (u32 indices, FP64 assembled values, FP32 copy for mixed)
@@ -120,6 +125,17 @@ struct KernelArgs {
     int n_rrows;
     const uint32_t *rrow, *rrow_ptr, *rrow_ids;
     unsigned long long *node_scale;
+
+    // DC continuation (src/analysis/dc.rs): 1 = on failure of the direct
+    // Newton solve, run source stepping (MOSFET circuits), GMIN stepping and
+    // pseudo-transient continuation on the device.  n_nodes: node rows come
+    // first (MNA order).  stampflag per row: bit 0 = its diagonal slot is
+    // written by the stamp map, bit 1 = its rhs entry is.  x_good: last
+    // converged continuation point (size n).
+    int continuation;
+    int n_nodes;
+    const uint8_t *stampflag;
+    double *x_good;
 
     // control
     int newton;                 // 1: Newton loop, 0: linear solve (+ refinement)
@@ -526,11 +542,29 @@ __device__ __forceinline__ int krylov_any(const KernelArgs &a, Team &g, double t
     return krylov<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
 }
 
-// The Newton loop (or a linear solve with refinement) for one system, run by
-// a team.  On return the leader thread has written `*info`; a false return
-// means a grid barrier gave up (nothing written).
+// One Newton run (or a linear solve with refinement).  RunCfg modifies the
+// system the way the reference's continuation steps do (gmin_newton_step,
+// dc.rs:297-330, and the rhs scalings of dc.rs:355-400 and :520-560):
+//   gshift  added to the diagonal of every node row,
+//   src     scale of the base rhs (the independent sources),
+//   pt      pseudo-transient anchor: b_i += pt * x_good_i on node rows.
+// The modifications are applied only when a.continuation is set.
+struct RunCfg {
+    double gshift, src, pt;
+    int max_outer, max_krylov;
+    bool trace;
+};
+
+struct RunOut {
+    int status, kcode, outer_done, err_iter, fallbacks, restarts;
+    long long kiters;
+    double last_dmax, bnorm_last, final_res;
+};
+
+// The Newton loop for one system, run by a team; results in `o` (identical in
+// every thread).  A false return means a grid barrier gave up.
 template <int LPR, class Team>
-__device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceInfo *info) {
+__device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const RunCfg &cfg, RunOut &o) {
     const int r0 = g.r0, r1 = g.r1, gtid = g.gtid, gstride = g.gstride;
 
     int status = kOk, kcode = kKrylovRunning, outer_done = 0, err_iter = 0;
@@ -539,7 +573,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
     double last_dmax = 0.0, bnorm_last = 0.0, final_res = -1.0;
     double fnorm_prev = -1.0, eta_prev = a.eta_max;
 
-    for (int outer = 0; outer < a.max_outer; ++outer) {
+    for (int outer = 0; outer < cfg.max_outer; ++outer) {
         // ---------------- device evaluation + stamping (Newton) ----------------
         if (a.newton) {
             const int ndev = a.nd + a.nq + a.nm;
@@ -570,12 +604,30 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 } else {
                     const int q = k - a.n_mslots;
                     const uint32_t row = a.rrow[q];
-                    double acc = a.base_b[row];
+                    double acc = cfg.src * a.base_b[row];
                     for (uint32_t j = a.rrow_ptr[q]; j < a.rrow_ptr[q + 1]; ++j) acc += a.rstamp[a.rrow_ids[j]];
                     a.b[row] = acc;
                 }
             }
             OHM_SYNC_OR(false);
+            if (a.continuation) {
+                // continuation terms on top of the assembled system; rows the
+                // stamp map does not write restart from their base values
+                for (int i = gtid; i < a.n; i += gstride) {
+                    const uint8_t f = a.stampflag[i];
+                    const bool node = i < a.n_nodes;
+                    const uint32_t ds = a.diag_slot[i];
+                    if (node && ds != kSentinel) {
+                        const double v = ((f & 1) ? a.vals64[ds] : a.base_vals[ds]) + cfg.gshift;
+                        a.vals64[ds] = v;
+                        if (a.vals32) a.vals32[ds] = (float)v;
+                    }
+                    double bv = (f & 2) ? a.b[i] : cfg.src * a.base_b[i];
+                    if (node && cfg.pt != 0.0) bv += cfg.pt * a.x_good[i];
+                    a.b[i] = bv;
+                }
+                OHM_SYNC_OR(false);
+            }
         }
 
         // -------------------------- FP64 residual r64 = b - A x -------------------------
@@ -650,25 +702,25 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
         KrylovOut ko{0, 0};
         int it32 = 0, it64 = 0;
         if (a.mixed) {
-            kcode = krylov_any<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, a.max_krylov), true, ko);
+            kcode = krylov_any<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, cfg.max_krylov), true, ko);
             if (kcode == kKrylovAbort) return false;
             it32 = ko.iterations;
             restarts += ko.restarts;
             if (kcode != kKrylovConverged) {
                 ++fallbacks;           // FP32 failed or stalled: redo this solve in FP64
-                kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
+                kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, cfg.max_krylov, false, ko);
                 if (kcode == kKrylovAbort) return false;
                 it64 = ko.iterations;
                 restarts += ko.restarts;
             }
         } else {
-            kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, a.max_krylov, false, ko);
+            kcode = krylov_any<double, LPR>(a, g, floor_tol, eta, cfg.max_krylov, false, ko);
             if (kcode == kKrylovAbort) return false;
             it64 = ko.iterations;
             restarts += ko.restarts;
         }
         kiters += it32 + it64;
-        if (a.trace && outer < a.trace_cap && g.leader()) {
+        if (cfg.trace && a.trace && outer < a.trace_cap && g.leader()) {
             double *tr = a.trace + (size_t)outer * kTraceCols;
             tr[0] = it32; tr[1] = it64; tr[2] = rnorm64; tr[3] = eta; tr[4] = -1.0; tr[5] = ko.restarts;
         }
@@ -716,11 +768,11 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
             if (!g.template allmax<3>(mx)) return false;
             last_dmax = mx[0];
             outer_done = outer + 1;
-            if (a.trace && outer < a.trace_cap && g.leader())
+            if (cfg.trace && a.trace && outer < a.trace_cap && g.leader())
                 a.trace[(size_t)outer * kTraceCols + 4] = mx[0];
             if (mx[2] > 0.0) { status = kErrNewtonNumerical; err_iter = outer; break; }
             if (mx[0] < a.abs_tol + a.rel_tol * mx[1]) { status = kOk; break; }
-            if (outer + 1 == a.max_outer) status = kErrNewtonNotConverged;
+            if (outer + 1 == cfg.max_outer) status = kErrNewtonNotConverged;
         }
     }
 
@@ -743,17 +795,160 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
         }
     }
 
+    o.status = status;
+    o.kcode = kcode;
+    o.outer_done = outer_done;
+    o.err_iter = err_iter;
+    o.fallbacks = fallbacks;
+    o.restarts = restarts;
+    o.kiters = kiters;
+    o.last_dmax = last_dmax;
+    o.bnorm_last = bnorm_last;
+    o.final_res = final_res;
+    return true;
+}
+
+// x[own rows] = src (or 0 when src is null), then a team sync.
+template <class Team>
+__device__ __forceinline__ bool team_copy(Team &g, double *dst, const double *src) {
+    for (int i = g.r0 + threadIdx.x; i < g.r1; i += blockDim.x) dst[i] = src ? src[i] : 0.0;
+    return g.sync();
+}
+
+// One system solved by a team: the direct Newton run (or linear solve), then,
+// when a.continuation is set and the direct run failed, the reference's
+// nonlinear DC strategy (run_nonlinear, src/analysis/dc.rs:60-290) on the
+// device: source stepping for circuits with MOSFETs (run_source_stepping,
+// :495-645: start at 0.1, grow by twice the last successful step, halve on
+// failure, at most 20 subdivisions), adaptive GMIN stepping (:160-253: from
+// 0.1, 1000x drops, 10x subdivisions from the last good level, at most 13),
+// a solve at the true GMIN, then pseudo-transient continuation from the last
+// GMIN point (:331-490: alpha from 0.1, 100x drops, at most 7 subdivisions,
+// b += alpha x_good on node rows) and a final true-DC solve.  The reference's
+// CPU sparse-LU retries have no counterpart.  The stages form a state machine
+// around one newton_run call site.  The leader writes `*info`; a false
+// return means a grid barrier gave up.
+template <int LPR, class Team>
+__device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceInfo *info) {
+    enum { kDirect, kSource, kGmin, kGminFinal, kPseudo, kPseudoFinal };
+    RunOut o;
+    RunCfg c{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, true};
+    int stage = kDirect, steps = 0, kind = kContNone, subdiv = 0;
+    bool have_good = false;
+    double last = 0.0, target = 0.0;
+    long long kiters = 0;
+    int fallbacks = 0, restarts = 0;
+    for (;;) {
+        if (!newton_run<LPR>(a, g, c, o)) return false;
+        kiters += o.kiters;
+        fallbacks += o.fallbacks;
+        restarts += o.restarts;
+        if (stage != kDirect) ++steps;
+        const bool ok = o.status == kOk;
+        bool finished = false, save_good = false;
+        int xsrc = -1;                  // next start: -1 keep x, 0 zeros, 1 x_good
+        switch (stage) {
+            case kDirect:
+                if (ok || !(a.newton && a.continuation)) { finished = true; break; }
+                have_good = false;
+                subdiv = 0;
+                xsrc = 0;
+                if (a.nm > 0) {
+                    stage = kSource; kind = kContSource; last = 0.0; target = 0.1;
+                    c = RunCfg{0.0, target, 0.0, 30, a.max_krylov, false};
+                } else {
+                    stage = kGmin; kind = kContGmin; last = 1.0; target = 1e-1;
+                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                }
+                break;
+            case kSource:
+                if (ok) {
+                    save_good = true;
+                    have_good = true;
+                    const double prev_step = target - last;
+                    last = target;
+                    subdiv = 0;
+                    if (fabs(target - 1.0) < 1e-12) { finished = true; break; }
+                    target = fmin(target + 2.0 * prev_step, 1.0);
+                    xsrc = -1;
+                    c.src = target;
+                    break;
+                }
+                target = last + 0.5 * (target - last);
+                if (++subdiv > 20 || target - last < 1e-6) {
+                    stage = kGmin; kind = kContGmin; have_good = false; subdiv = 0; last = 1.0; target = 1e-1;
+                    xsrc = 0;
+                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                } else {
+                    xsrc = have_good ? 1 : 0;
+                    c.src = target;
+                }
+                break;
+            case kGmin:
+                if (ok) {
+                    save_good = true;
+                    have_good = true;
+                    last = target;
+                    subdiv = 0;
+                    target *= 1e-3;
+                } else {
+                    if (++subdiv > 13) { finished = true; break; }
+                    target = last * pow(10.0, -(double)subdiv);
+                }
+                xsrc = have_good ? 1 : 0;
+                if (target > 1e-13) {
+                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                } else {
+                    stage = kGminFinal;
+                    c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+                }
+                break;
+            case kGminFinal:
+                if (ok || !have_good) { finished = true; break; }
+                stage = kPseudo; kind = kContPseudo; last = 1.0; target = 1e-1; subdiv = 0;
+                xsrc = 1;
+                c = RunCfg{target, 1.0, target, 20, a.max_krylov, false};
+                break;
+            case kPseudo:
+                if (ok) {
+                    save_good = true;
+                    last = target;
+                    subdiv = 0;
+                    target *= 1e-2;
+                } else {
+                    if (++subdiv > 7) { finished = true; break; }
+                    target = last * pow(10.0, -(double)subdiv);
+                }
+                xsrc = 1;
+                if (target > 1e-8) {
+                    c = RunCfg{target, 1.0, target, 20, a.max_krylov, false};
+                } else {
+                    stage = kPseudoFinal;
+                    c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+                }
+                break;
+            default:
+                finished = true;
+                break;
+        }
+        if (save_good && !team_copy(g, a.x_good, a.x)) return false;
+        if (finished) break;
+        if (xsrc == 0 && !team_copy(g, a.x, (const double *)nullptr)) return false;
+        if (xsrc == 1 && !team_copy(g, a.x, a.x_good)) return false;
+    }
     if (g.leader()) {
-        info->status = status;
-        info->krylov_code = kcode;
-        info->iterations = outer_done;
-        info->error_iteration = err_iter;
+        info->status = o.status;
+        info->krylov_code = o.kcode;
+        info->iterations = o.outer_done;
+        info->error_iteration = o.err_iter;
         info->krylov_iterations = kiters;
         info->fp64_fallbacks = fallbacks;
         info->krylov_restarts = restarts;
-        info->max_residual = last_dmax;
-        info->final_residual = final_res;
-        info->b_norm = bnorm_last;
+        info->max_residual = o.last_dmax;
+        info->final_residual = o.final_res;
+        info->b_norm = o.bnorm_last;
+        info->continuation_steps = steps;
+        info->continuation_kind = kind;
     }
     return true;
 }

@@ -117,6 +117,8 @@ class NewtonParams:
     forcing: int = 0              # 0 constant inner_rtol, 1 Eisenstat-Walker
     eta_max: float = 0.5
     fp32_max_iterations: int = 600
+    continuation: bool = False    # reference DC strategy on failure (src/analysis/dc.rs:60-290)
+    n_nodes: int = 0              # node rows; filled from the system by NewtonPlan / NewtonBatch
 
     def to_c(self):
         p = _lib.NewtonParamsC()
@@ -129,6 +131,8 @@ class NewtonParams:
                                   fp32_max_iterations=self.fp32_max_iterations).to_c()
         p.forcing = int(self.forcing)
         p.eta_max = float(self.eta_max)
+        p.continuation = 1 if self.continuation else 0
+        p.n_nodes = int(self.n_nodes)
         keep = None
         if self.initial_guess is not None:
             keep = np.ascontiguousarray(self.initial_guess, dtype=np.float64)
@@ -294,6 +298,8 @@ class NewtonPlan:
     def newton_device(self, x_dev_ptr: int, params: NewtonParams | None = None) -> dict:
         """Run Newton on a device vector (raw CUDA pointer, e.g. torch ``data_ptr()``)."""
         p, keep = (params or NewtonParams()).to_c()
+        if p.continuation and p.n_nodes <= 0:
+            p.n_nodes = int(self.sysm.n_nodes)
         info = _lib.SolveInfo()
         st = self.ctx.lib.ohm_plan_newton_device(self._h, C.c_void_p(int(x_dev_ptr)), C.byref(p),
                                                  C.byref(info))
@@ -374,11 +380,12 @@ class NewtonBatch:
                 vaf = v
         rp = np.ascontiguousarray(rp)
         ci = np.ascontiguousarray(ci)
+        self.n_nodes = np.array([int(s.n_nodes) for s in systems], dtype=np.int32)
         h = C.c_void_p()
         st = self.ctx.lib.ohm_batch_create(
             self.ctx.handle, self.n_instances, vptr(self.row_off), vptr(self.nnz_off), u32ptr(rp), u32ptr(ci),
             dptr(vals), dptr(bb), vptr(doff), vptr(dd), vptr(qoff), vptr(qd),
-            None if vaf is None else dptr(vaf), vptr(moff), vptr(md), C.byref(h))
+            None if vaf is None else dptr(vaf), vptr(moff), vptr(md), vptr(self.n_nodes), C.byref(h))
         if st != _lib.OK:
             _raise(st)
         self._h = h
