@@ -290,6 +290,18 @@ ohm_status ohm_batch_newton_device(ohm_batch *batch, double *x_inout_device, con
                                    ohm_solve_info *summary);
 /* Per-instance results of the last ohm_batch_newton_device call. */
 ohm_status ohm_batch_instance_info(ohm_batch *batch, ohm_solve_info *infos, int64_t n_instances);
+/* Autotuner: times the batch kernel variants (lanes per row around the
+ * density heuristic x launch shapes (256 threads, 2 blocks/SM), (256, 4),
+ * (128, 8)) on `sample_size` instances (<= 0: 512) spread over the size
+ * distribution, three Newton iterations with `params` from zero (no
+ * continuation), and keeps the fastest for later ohm_batch_newton_device
+ * calls.  Outputs may be NULL. */
+ohm_status ohm_batch_autotune(ohm_batch *batch, const ohm_newton_params *params, int32_t sample_size,
+                              int32_t *lanes_per_row, int32_t *threads_per_block, int32_t *blocks_per_sm,
+                              double *sample_ms);
+/* Choose the kernel variant directly (same choices as the autotuner). */
+ohm_status ohm_batch_set_kernel(ohm_batch *batch, int32_t lanes_per_row, int32_t threads_per_block,
+                                int32_t blocks_per_sm);
 
 #ifdef __cplusplus
 }

@@ -94,6 +94,9 @@ SIGNATURES = {
     "ohm_batch_create": (C.c_int, [_vp, _i64, _vp, _vp, _u32p, _u32p, _dp, _dp, _vp, _vp, _vp, _vp, _dp,
                                    _vp, _vp, _vp, C.POINTER(_vp)]),
     "ohm_batch_destroy": (C.c_int, [_vp]),
+    "ohm_batch_autotune": (C.c_int, [_vp, C.POINTER(NewtonParamsC), C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "ohm_batch_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),
     "ohm_isai_apply": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64]),
     "ohm_batch_newton_device": (C.c_int, [_vp, _vp, C.POINTER(NewtonParamsC), C.POINTER(SolveInfo)]),
     "ohm_batch_instance_info": (C.c_int, [_vp, C.POINTER(SolveInfo), _i64]),

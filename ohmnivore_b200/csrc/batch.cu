@@ -11,124 +11,19 @@
 #include <numeric>
 #include <vector>
 
+#include "batch_kernel.cuh"
 #include "host_util.h"
 
 using namespace ohm;
 
-namespace {
-
-constexpr int kBatchBlock = 256;
-
-struct BatchArgs {
-    KernelArgs base;                // pointers to the packed arrays, shared scalars
-    int n_inst;
-    const int64_t *row_off, *nnz_off;
-    const int64_t *d_off, *q_off, *m_off;      // device descriptor offsets
-    const int64_t *ms_off, *mid_off, *rs_off, *rid_off;   // stamp-map offsets
-    const int32_t *order;           // instances by decreasing nnz
-    unsigned int *queue;            // next position in `order`
-    DeviceInfo *infos;              // per instance
-    double *node_scale_base;        // per row (8 bytes)
-    const int32_t *n_nodes;         // per instance (continuation), may be null
-    const uint8_t *stampflag;       // per row
-    double *x_good;                 // per row
-};
-
-template <typename P>
-__device__ __forceinline__ P *offset(P *p, int64_t k) { return p ? p + k : p; }
-
-template <int LPR>
-__global__ void __launch_bounds__(kBatchBlock) batch_solver(BatchArgs B) {
-    __shared__ double smem[32 * 4];
-    __shared__ int s_q;
-    for (;;) {
-        if (threadIdx.x == 0) s_q = (int)atomicAdd(B.queue, 1u);
-        __syncthreads();
-        const int q = s_q;
-        __syncthreads();
-        if (q >= B.n_inst) return;
-        const int i = B.order[q];
-        const int64_t ro = B.row_off[i], no = B.nnz_off[i];
-        const int64_t dq = B.d_off[i], qq = B.q_off[i], mq = B.m_off[i];
-        KernelArgs a = B.base;
-        a.n = (int)(B.row_off[i + 1] - ro);
-        a.nnz = (int)(B.nnz_off[i + 1] - no);
-        a.row_ptr = B.base.row_ptr + ro + i;               // n_i + 1 local row pointers
-        a.col = B.base.col + no;
-        a.vals64 = B.base.vals64 + no;
-        a.vals32 = offset(B.base.vals32, no);
-        a.base_vals = B.base.base_vals + no;
-        a.base_b = B.base.base_b + ro;
-        a.b = B.base.b + ro;
-        a.x = B.base.x + ro;
-        a.x_prev = B.base.x_prev + ro;
-        a.r64 = B.base.r64 + ro;
-        a.dx = B.base.dx + ro;
-        a.partner = B.base.partner + ro;
-        a.diag_slot = B.base.diag_slot + ro;
-        a.off_slot = B.base.off_slot + ro;
-        a.rowflag = offset(B.base.rowflag, ro);
-        a.pc_part = (double *)B.base.pc_part + ro;
-        a.rec0 = (double *)B.base.rec0 + 4 * ro;
-        a.rec1 = (double *)B.base.rec1 + 4 * ro;
-        a.rhat = (double *)B.base.rhat + ro;
-        a.s = (double *)B.base.s + ro;
-        a.t = (double *)B.base.t + ro;
-        a.phat = (double *)B.base.phat + ro;
-        a.shat = (double *)B.base.shat + ro;
-        a.d = (double *)B.base.d + ro;
-        a.nd = (int)(B.d_off[i + 1] - dq);
-        a.nq = (int)(B.q_off[i + 1] - qq);
-        a.nm = (int)(B.m_off[i + 1] - mq);
-        a.diodes = B.base.diodes + dq;
-        a.bjts = B.base.bjts + qq;
-        a.mosfets = B.base.mosfets + mq;
-        a.bjt_vaf = offset(B.base.bjt_vaf, qq);
-        a.mstamp = B.base.mstamp + 4 * dq + 9 * qq + 6 * mq;
-        a.rstamp = B.base.rstamp + 2 * dq + 3 * qq + 2 * mq;
-        a.n_mslots = (int)(B.ms_off[i + 1] - B.ms_off[i]);
-        a.mslot = B.base.mslot + B.ms_off[i];
-        a.mslot_ptr = B.base.mslot_ptr + B.ms_off[i] + i;
-        a.mslot_ids = B.base.mslot_ids + B.mid_off[i];
-        a.n_rrows = (int)(B.rs_off[i + 1] - B.rs_off[i]);
-        a.rrow = B.base.rrow + B.rs_off[i];
-        a.rrow_ptr = B.base.rrow_ptr + B.rs_off[i] + i;
-        a.rrow_ids = B.base.rrow_ids + B.rid_off[i];
-        a.node_scale = (unsigned long long *)(B.node_scale_base + ro);
-        a.trace = nullptr;
-        a.n_nodes = B.n_nodes ? B.n_nodes[i] : 0;
-        a.stampflag = B.stampflag + ro;
-        a.x_good = B.x_good + ro;
-        BlockTeam g;
-        g.r0 = 0;
-        g.r1 = a.n;
-        g.gtid = threadIdx.x;
-        g.gstride = blockDim.x;
-        g.smem = smem;
-        solve_body<LPR>(a, g, &B.infos[i]);
-        __syncthreads();
-    }
-}
-
-using BatchFn = void (*)(BatchArgs);
-
-BatchFn pick(int lpr) {
-    switch (lpr) {
-        case 1: return batch_solver<1>;
-        case 2: return batch_solver<2>;
-        case 4: return batch_solver<4>;
-        case 8: return batch_solver<8>;
-        default: return batch_solver<16>;
-    }
-}
-
-}  // namespace
-
 struct ohm_batch {
     ohm_ctx *ctx = nullptr;
     int64_t n_inst = 0, rows = 0, nnz = 0, nd = 0, nq = 0, nm = 0;
-    int lpr = 2;
+    int lpr = 2, shape = 0;             // kernel choice (ohm_batch_autotune)
     std::vector<void *> allocs;
+    int32_t *order = nullptr;           // instances by decreasing nnz
+    int32_t *sample = nullptr;          // autotune sample (capacity n_inst)
+    double *x_tune = nullptr;           // autotune scratch solution
     BatchArgs args{};
     std::vector<DeviceInfo> host_infos;
     DeviceInfo *infos = nullptr;
@@ -246,7 +141,7 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     b->ctx = c;
     b->n_inst = n_inst; b->rows = rows; b->nnz = nnz; b->nd = nd; b->nq = nq; b->nm = nm;
     const double avg = (double)nnz / (double)rows;
-    b->lpr = avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : (avg <= 24.0 ? 8 : 16)));
+    b->lpr = avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : 8));
     KernelArgs &a = b->args.base;
     a = KernelArgs{};
     uint32_t *u32 = nullptr;
@@ -300,7 +195,8 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     PUT(i64, mid_off.data(), n_inst + 1); b->args.mid_off = i64;
     PUT(i64, rs_off.data(), n_inst + 1); b->args.rs_off = i64;
     PUT(i64, rid_off.data(), n_inst + 1); b->args.rid_off = i64;
-    PUT(i32, order.data(), n_inst); b->args.order = i32;
+    PUT(i32, order.data(), n_inst); b->args.order = i32; b->order = i32;
+    ZERO(b->sample, n_inst);
     ZERO(b->infos, n_inst);
     ZERO(b->queue, 4);
 #undef PUT
@@ -332,8 +228,8 @@ extern "C" ohm_status ohm_batch_destroy(ohm_batch *b) {
     return OHM_OK;
 }
 
-extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const ohm_newton_params *np,
-                                              ohm_solve_info *summary) {
+// Validated kernel arguments of one batched Newton call.
+static ohm_status batch_args(ohm_batch *b, double *x_dev, const ohm_newton_params *np, BatchArgs &B) {
     if (!b || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
     if (np->max_iterations <= 0) return ohm_fail(OHM_ERR_NEWTON_NOT_CONVERGED, "Newton solver did not converge after 0 iterations");
     ohm_status st = ohm_check_krylov(&np->krylov);
@@ -342,9 +238,7 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
         return ohm_fail(OHM_ERR_INVALID_ARG, "batched solves use block Jacobi (ISAI(1) is for single systems)");
     if (np->continuation && !b->args.n_nodes)
         return ohm_fail(OHM_ERR_INVALID_ARG, "continuation needs the per-instance n_nodes given at creation");
-    ohm_ctx *c = b->ctx;
-    CUDA_TRY(cudaSetDevice(c->device));
-    BatchArgs B = b->args;
+    B = b->args;
     KernelArgs &a = B.base;
     a.x = x_dev;
     a.precond = np->krylov.precond == OHM_PRECOND_NONE ? kPcNone
@@ -365,17 +259,39 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
                                                                : np->krylov.max_iterations;
     a.max_restarts = std::max(0, np->krylov.max_restarts);
     a.continuation = np->continuation ? 1 : 0;
+    return OHM_OK;
+}
+
+// One launch over `n` instances listed in `order` (device): a persistent grid
+// of (blocks per SM) x SMs blocks, each taking instances from the queue.
+static ohm_status launch_batch(ohm_batch *b, BatchArgs B, int lpr, int shape, int n, const int32_t *order) {
+    ohm_ctx *c = b->ctx;
+    B.order = order;
+    B.n_inst = n;
+    BatchFn fn = batch_kernel(lpr, shape);
+    const int block = kBatchShapes[shape].block;
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0));
+    if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "batch kernel does not fit on an SM");
+    const int grid = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, n);
+    CUDA_TRY(cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), c->stream));
+    fn<<<grid, block, 0, c->stream>>>(B);
+    CUDA_TRY(cudaGetLastError());
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const ohm_newton_params *np,
+                                              ohm_solve_info *summary) {
+    BatchArgs B;
+    ohm_status st = batch_args(b, x_dev, np, B);
+    if (st != OHM_OK) return st;
+    ohm_ctx *c = b->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
     if (np->initial_guess)
         CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, b->rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), c->stream));
     CUDA_TRY(cudaMemsetAsync(b->infos, 0, b->n_inst * sizeof(DeviceInfo), c->stream));
-    BatchFn fn = pick(b->lpr);
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchBlock, 0));
-    if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "batch kernel does not fit on an SM");
-    const int grid = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, b->n_inst);
-    fn<<<grid, kBatchBlock, 0, c->stream>>>(B);
-    CUDA_TRY(cudaGetLastError());
+    st = launch_batch(b, B, b->lpr, b->shape, (int)b->n_inst, b->order);
+    if (st != OHM_OK) return st;
     CUDA_TRY(cudaMemcpyAsync(b->host_infos.data(), b->infos, b->n_inst * sizeof(DeviceInfo), cudaMemcpyDeviceToHost,
                              c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -432,5 +348,82 @@ extern "C" ohm_status ohm_batch_instance_info(ohm_batch *b, ohm_solve_info *info
         o.continuation_steps = d.continuation_steps;
         o.continuation_kind = d.continuation_kind;
     }
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_autotune(ohm_batch *b, const ohm_newton_params *np, int32_t sample_size,
+                                         int32_t *lanes_per_row, int32_t *threads_per_block,
+                                         int32_t *blocks_per_sm, double *sample_ms) {
+    if (!b || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_ctx *c = b->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!b->x_tune) {
+        cudaError_t e = b->zero(&b->x_tune, (size_t)b->rows);
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "autotune scratch: %s", cudaGetErrorString(e));
+    }
+    BatchArgs B;
+    ohm_status st = batch_args(b, b->x_tune, np, B);
+    if (st != OHM_OK) return st;
+    // a few Newton iterations show each variant's throughput; the
+    // continuation (whose length depends on the path) stays off
+    B.base.max_outer = std::min(B.base.max_outer, 3);
+    B.base.continuation = 0;
+    // sample: every k-th instance of the largest-first order, so the sample
+    // spans the size distribution
+    const int64_t n = b->n_inst;
+    const int64_t m = sample_size <= 0 ? std::min<int64_t>(n, 512) : std::min<int64_t>(n, sample_size);
+    std::vector<int32_t> order(n), pick(m);
+    CUDA_TRY(cudaMemcpyAsync(order.data(), b->order, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int64_t k = 0; k < m; ++k) pick[k] = order[(k * n) / m];
+    CUDA_TRY(cudaMemcpyAsync(b->sample, pick.data(), m * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    // candidates: lanes per row around the density heuristic, every shape
+    const int base = b->lpr;
+    std::vector<int> lprs = {base};
+    if (base > 1) lprs.push_back(base / 2);
+    if (base < 8) lprs.push_back(base * 2);
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = -1.0f;
+    int best_lpr = b->lpr, best_shape = b->shape;
+    for (int lpr : lprs) {
+        for (int sh = 0; sh < kNumBatchShapes; ++sh) {
+            cudaMemsetAsync(b->x_tune, 0, b->rows * sizeof(double), c->stream);
+            cudaEventRecord(e0, c->stream);
+            st = launch_batch(b, B, lpr, sh, (int)m, b->sample);
+            if (st != OHM_OK) break;
+            cudaEventRecord(e1, c->stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) { st = ohm_fail(OHM_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
+            if (best < 0.0f || ms < best) { best = ms; best_lpr = lpr; best_shape = sh; }
+        }
+        if (st != OHM_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != OHM_OK) return st;
+    b->lpr = best_lpr;
+    b->shape = best_shape;
+    if (lanes_per_row) *lanes_per_row = best_lpr;
+    if (threads_per_block) *threads_per_block = kBatchShapes[best_shape].block;
+    if (blocks_per_sm) *blocks_per_sm = kBatchShapes[best_shape].min_blocks;
+    if (sample_ms) *sample_ms = best;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_set_kernel(ohm_batch *b, int32_t lanes_per_row, int32_t threads_per_block,
+                                           int32_t blocks_per_sm) {
+    if (!b) return ohm_fail(OHM_ERR_INVALID_ARG, "null batch");
+    int shape = -1;
+    for (int k = 0; k < kNumBatchShapes; ++k)
+        if (kBatchShapes[k].block == threads_per_block && kBatchShapes[k].min_blocks == blocks_per_sm) shape = k;
+    if (!(lanes_per_row == 1 || lanes_per_row == 2 || lanes_per_row == 4 || lanes_per_row == 8) || shape < 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG,
+                        "lanes_per_row must be 1, 2, 4 or 8; (threads, blocks per SM) one of (256,2), (256,4), (128,8)");
+    b->lpr = lanes_per_row;
+    b->shape = shape;
     return OHM_OK;
 }

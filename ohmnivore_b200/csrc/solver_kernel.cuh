@@ -815,6 +815,13 @@ __device__ __forceinline__ bool team_copy(Team &g, double *dst, const double *sr
     return g.sync();
 }
 
+// BiCGSTAB cap of an intermediate continuation step: the reference's
+// fail-fast limits (dc.rs:171-174, :391-393, :531-536), scaled by 4 for the
+// tighter inner tolerance used here, never above the caller's limit.
+__device__ __forceinline__ int cont_cap(const KernelArgs &a, int reference_cap) {
+    return min(a.max_krylov, 4 * reference_cap);
+}
+
 // One system solved by a team: the direct Newton run (or linear solve), then,
 // when a.continuation is set and the direct run failed, the reference's
 // nonlinear DC strategy (run_nonlinear, src/analysis/dc.rs:60-290) on the
@@ -855,10 +862,10 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 xsrc = 0;
                 if (a.nm > 0) {
                     stage = kSource; kind = kContSource; last = 0.0; target = 0.1;
-                    c = RunCfg{0.0, target, 0.0, 30, a.max_krylov, false};
+                    c = RunCfg{0.0, target, 0.0, 30, cont_cap(a, 200), false};
                 } else {
                     stage = kGmin; kind = kContGmin; last = 1.0; target = 1e-1;
-                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                    c = RunCfg{target, 1.0, 0.0, 15, cont_cap(a, 300), false};
                 }
                 break;
             case kSource:
@@ -878,7 +885,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 if (++subdiv > 20 || target - last < 1e-6) {
                     stage = kGmin; kind = kContGmin; have_good = false; subdiv = 0; last = 1.0; target = 1e-1;
                     xsrc = 0;
-                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                    c = RunCfg{target, 1.0, 0.0, 15, cont_cap(a, 300), false};
                 } else {
                     xsrc = have_good ? 1 : 0;
                     c.src = target;
@@ -897,7 +904,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 }
                 xsrc = have_good ? 1 : 0;
                 if (target > 1e-13) {
-                    c = RunCfg{target, 1.0, 0.0, 15, a.max_krylov, false};
+                    c = RunCfg{target, 1.0, 0.0, 15, cont_cap(a, 300), false};
                 } else {
                     stage = kGminFinal;
                     c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
@@ -907,7 +914,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 if (ok || !have_good) { finished = true; break; }
                 stage = kPseudo; kind = kContPseudo; last = 1.0; target = 1e-1; subdiv = 0;
                 xsrc = 1;
-                c = RunCfg{target, 1.0, target, 20, a.max_krylov, false};
+                c = RunCfg{target, 1.0, target, 20, cont_cap(a, 500), false};
                 break;
             case kPseudo:
                 if (ok) {
@@ -921,7 +928,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 }
                 xsrc = 1;
                 if (target > 1e-8) {
-                    c = RunCfg{target, 1.0, target, 20, a.max_krylov, false};
+                    c = RunCfg{target, 1.0, target, 20, cont_cap(a, 500), false};
                 } else {
                     stage = kPseudoFinal;
                     c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};

@@ -419,6 +419,26 @@ class NewtonBatch:
             _raise(st, info)
         return self.last_info
 
+    def autotune(self, params: NewtonParams | None = None, sample_size: int = 0) -> dict:
+        """Pick the fastest kernel variant on a sample of the batch (kept for
+        later ``newton_device`` calls)."""
+        p, keep = (params or NewtonParams()).to_c()
+        lpr, tpb, bps = C.c_int32(), C.c_int32(), C.c_int32()
+        ms = C.c_double()
+        st = self.ctx.lib.ohm_batch_autotune(self._h, C.byref(p), int(sample_size), C.byref(lpr), C.byref(tpb),
+                                             C.byref(bps), C.byref(ms))
+        del keep
+        if st:
+            _raise(st)
+        return {"lanes_per_row": lpr.value, "threads_per_block": tpb.value, "blocks_per_sm": bps.value,
+                "sample_ms": ms.value}
+
+    def set_kernel(self, lanes_per_row: int, threads_per_block: int, blocks_per_sm: int):
+        st = self.ctx.lib.ohm_batch_set_kernel(self._h, int(lanes_per_row), int(threads_per_block),
+                                               int(blocks_per_sm))
+        if st:
+            _raise(st)
+
     def instance_info(self):
         arr = (_lib.SolveInfo * self.n_instances)()
         st = self.ctx.lib.ohm_batch_instance_info(self._h, arr, self.n_instances)

@@ -148,3 +148,38 @@ def test_batch_rejects_bad_instance(ctx):
     bad.diode_descriptors["g_row_col"][0, 0] = bad.g.nnz + 3
     with pytest.raises(S.CompileError):
         S.NewtonBatch([s, bad], ctx)
+
+
+def test_batch_kernel_variants_agree(ctx):
+    """Every kernel variant the autotuner can choose (lanes per row x launch
+    shape) converges to the same operating points.  The variants reduce in
+    different orders, so an instance's Krylov path can differ (and break
+    down in one variant but not another); continuation is on, as in use."""
+    systems = [mna.compile_circuit(c) for c in ck.monte_carlo_batch(12, seed=4, n_lo=50, n_hi=400)]
+    batch = S.NewtonBatch(systems, ctx)
+    try:
+        ref, _ = _solve(batch, params=_params(0, continuation=True))
+        for lpr in (1, 2, 4, 8):
+            for tpb, bps in ((256, 2), (256, 4), (128, 8)):
+                batch.set_kernel(lpr, tpb, bps)
+                x, _ = _solve(batch, params=_params(0, continuation=True))
+                assert _rel(x, ref) < 1e-9, (lpr, tpb, bps)
+        with pytest.raises(S.InvalidArgument):
+            batch.set_kernel(3, 256, 2)
+    finally:
+        batch.close()
+
+
+def test_batch_autotune(ctx):
+    systems = [mna.compile_circuit(c) for c in ck.monte_carlo_batch(40, seed=6, n_lo=50, n_hi=800)]
+    batch = S.NewtonBatch(systems, ctx)
+    try:
+        choice = batch.autotune(_params(0, continuation=True), sample_size=16)
+        assert choice["lanes_per_row"] in (1, 2, 4, 8)
+        assert (choice["threads_per_block"], choice["blocks_per_sm"]) in ((256, 2), (256, 4), (128, 8))
+        assert choice["sample_ms"] > 0
+        x, info = _solve(batch, params=_params(0, continuation=True))
+    finally:
+        batch.close()
+    assert info["status"] == 0
+    _check_all(systems, batch.split(x))
