@@ -44,6 +44,10 @@ def parse():
     p.add_argument("--rows", type=int, default=500)
     p.add_argument("--cols", type=int, default=500)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--batch", type=int, default=4096,
+                   help="Monte Carlo batch size for the batched measurement (0 skips it)")
+    p.add_argument("--batch-mixed", action="store_true",
+                   help="also time the batch with the FP32 Krylov bulk")
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                    help="one warm-up and one timed solve only (for an ncu capture)")
     return p.parse_args()
@@ -347,12 +351,118 @@ def main():
         line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
                                 "sample": f"1 full DC solve of the workload ({it_ref} FP64 Newton "
                                           "iterations, SuperLU per iteration), single thread"}
+    if args.batch > 0:
+        line["batch"] = batch_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def batch_params(mixed: bool):
+    """Monte Carlo batch: Newton to max|dx| < 1e-10 V, constant inner
+    tolerance 1e-4 on the scaled residual, DC continuation on failure."""
+    from ohmnivore_b200 import solver as S
+    return S.NewtonParams(max_iterations=100, abs_tol=1e-10, bicgstab_max_iterations=20000,
+                          bicgstab_tolerance=1e-14, precision=1 if mixed else 0, inner_rtol=1e-4,
+                          continuation=True)
+
+
+def batch_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """Batched Monte Carlo DC (BJT differential-pair meshes, 50-20,000
+    nodes, seed 3, VAF 100 V): one launch over the packed batch, against the
+    plain FP64 single-circuit path on a size-stratified sample, and the
+    error of a sample against the FP64 oracle."""
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    t0 = time.perf_counter()
+    systems = [mna.compile_circuit(c) for c in circuits.monte_carlo_batch(args.batch, seed=3, vaf=100.0)]
+    setup_s = time.perf_counter() - t0
+    batch = S.NewtonBatch(systems, ctx)
+    rows = batch.rows
+    nnz = int(batch.nnz_off[-1])
+    x = torch.zeros(rows, dtype=torch.float64, device=f"cuda:{local_rank}")
+    t0 = time.perf_counter()
+    choice = batch.autotune(batch_params(False), sample_size=256)
+    tune_s = time.perf_counter() - t0
+
+    def timed(mixed):
+        with torch.cuda.stream(stream):
+            x.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        info = batch.newton_device(x.data_ptr(), batch_params(mixed), check=False)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=x.device)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), info
+
+    with ClockSampler(local_rank) as clk:
+        ms, info = timed(False)
+    per = batch.instance_info()
+    failed = sum(1 for q in per if q["status"] != 0)
+    out = {"workload": f"Monte Carlo batch: {args.batch} BJT differential-pair meshes, 50-20,000 nodes "
+                       f"(seed 3, VAF 100 V), {rows} unknowns, {nnz} nonzeros",
+           "value": world * args.batch / (ms * 1e-3), "unit": "solves/s", "ms": ms,
+           "precision": "FP64", "kernel_launches": 1, "failed_instances": failed,
+           "continuation_instances": sum(1 for q in per if q["continuation_steps"] > 0),
+           "krylov_iterations": info["krylov_iterations"], "autotune": choice,
+           "autotune_s": tune_s, "host_setup_s": setup_s, "clocks": clk.summary()}
+    xs = batch.split(x.cpu().numpy())
+    if args.batch_mixed:
+        ms_m, info_m = timed(True)
+        per_m = batch.instance_info()
+        out["mixed_precision"] = {"value": world * args.batch / (ms_m * 1e-3), "ms": ms_m,
+                                  "failed_instances": sum(1 for q in per_m if q["status"] != 0),
+                                  "fp64_fallbacks": info_m["fp64_fallbacks"]}
+    batch.close()
+
+    # plain FP64 one-circuit-at-a-time GPU path on a size-stratified sample
+    order = np.argsort([-s.size for s in systems], kind="stable")
+    sample = [int(order[(k * len(order)) // 32]) for k in range(32)]
+    single_ms = 0.0
+    for i in sample:
+        s = systems[i]
+        plan = S.NewtonPlan(s, ctx)
+        xi = torch.zeros(s.size, dtype=torch.float64, device=x.device)
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        try:
+            plan.newton_device(xi.data_ptr(), batch_params(False))
+        except S.OhmnivoreError:
+            pass
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        single_ms += e0.elapsed_time(e1)
+        plan.close()
+    single_rate = len(sample) / (single_ms * 1e-3)
+    out["single_fp64"] = {"value": world * single_rate, "unit": "solves/s",
+                          "sample": "32 instances, every 128th by size, one persistent-kernel solve each"}
+    out["batched_vs_single"] = out["value"] / (world * single_rate)
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import newton_ref
+        ev, ei = 0.0, 0.0
+        for i in sample[::2]:
+            s = systems[i]
+            ref, _ = newton_ref.dc_operating_point(s)
+            nn = slice(0, s.n_nodes)
+            br = slice(s.n_nodes, s.size)
+            ev = max(ev, float(np.max(np.abs(xs[i][nn] - ref[nn])) / np.max(np.abs(ref[nn]))))
+            if s.size > s.n_nodes:
+                ei = max(ei, float(np.max(np.abs(xs[i][br] - ref[br])) / max(np.max(np.abs(ref[br])), 1e-300)))
+        out["rel_err_vs_oracle"] = {"voltages": ev, "currents": ei, "instances": len(sample[::2])}
+    return out
 
 
 def run_profile_case(args):
