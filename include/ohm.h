@@ -256,6 +256,70 @@ ohm_status ohm_plan_assemble(ohm_plan *plan, const double *x_host, double *value
 /* One limiting step: x_new_inout (host) is damped against x_old (host). */
 ohm_status ohm_plan_limit(ohm_plan *plan, const double *x_old_host, double *x_new_inout);
 
+/* -------------------------------------------------------------- transient --
+ * Fixed-step backward-Euler transient with a Newton solve per step, run on
+ * the device.  The reference's transient (src/analysis/transient.rs:25-210)
+ * is linear only: it forms A = G + C/h and b = b(t_n) + (C/h) x_{n-1} per BE
+ * step (:285-333) and ignores nonlinear devices; this engine uses the same
+ * companion system as the base of a Newton solve (device evaluation and
+ * stamping on top of it) at every step.  Its adaptive BE/TRAP step control
+ * (:84-178) is not implemented: the step is fixed.
+ *
+ * Time-dependent sources (collect_source_info / evaluate_b_at_time,
+ * transient.rs:212-280, and transient_source.rs:8-118): b(t) is the sum over
+ * sources of sign * value(t) at their rhs rows; a source without a transient
+ * function contributes its DC value. */
+typedef enum {
+    OHM_TRAN_DC = -1,
+    OHM_TRAN_PULSE = 0,   /* p = v1, v2, td, tr, tf, pw, per */
+    OHM_TRAN_SIN = 1,     /* p = vo, va, freq, td, theta */
+    OHM_TRAN_PWL = 2,     /* (t, v) pairs at pwl_points[2*pwl_offset ...] */
+    OHM_TRAN_EXP = 3      /* p = v1, v2, td1, tau1, td2, tau2 */
+} ohm_tran_kind;
+
+typedef struct {
+    int32_t kind;                /* ohm_tran_kind */
+    int32_t n_rows;              /* rhs entries: 1 (voltage source branch) or 1-2 (current source) */
+    uint32_t rows[2];
+    double sign[2];
+    double dc;                   /* value of an OHM_TRAN_DC source */
+    double p[7];
+    int32_t pwl_offset, pwl_count;
+} ohm_source;
+
+typedef struct {
+    int32_t status;              /* ohm_status of the run */
+    int32_t steps_done;          /* accepted steps */
+    int32_t failed_step;         /* step whose Newton solve failed, -1 if none */
+    int32_t krylov_code;
+    int64_t newton_iterations;   /* over all steps */
+    int64_t krylov_iterations;
+    int32_t fp64_fallbacks;
+    int32_t launches;            /* kernel launches (one per steps_per_launch steps) */
+    int32_t graph;               /* 1: the launches ran as one CUDA graph */
+    int32_t reserved;
+    double max_residual;         /* max|dx| of the last Newton iteration of a failed step */
+} ohm_transient_info;
+
+typedef struct ohm_transient ohm_transient;
+/* C: capacitance / inductance matrix in its own CSR (n rows, the plan's size);
+ * each of its entries must lie on the plan's conductance pattern.  probes:
+ * rows of x recorded after every step. */
+ohm_status ohm_transient_create(ohm_plan *plan, int64_t c_nnz, const uint32_t *c_row_ptr, const uint32_t *c_col,
+                                const double *c_values, const ohm_source *sources, int32_t n_sources,
+                                const double *pwl_points, int32_t n_pwl_points, const uint32_t *probe_rows,
+                                int32_t n_probes, ohm_transient **out);
+ohm_status ohm_transient_destroy(ohm_transient *tr);
+/* n_steps BE steps of size h from t0: x_inout_device holds x(t0) (e.g. the DC
+ * operating point) and receives x(t0 + n_steps h).  Each launch runs
+ * steps_per_launch steps in one persistent kernel; use_graph = 1 records
+ * the launches (and the waveform download) as one CUDA graph and replays it.
+ * waveforms_host (may be NULL): n_steps x n_probes doubles, row-major.  The
+ * plan's assembled system is restored to its base afterwards. */
+ohm_status ohm_transient_run(ohm_transient *tr, double *x_inout_device, double t0, double h, int32_t n_steps,
+                             int32_t steps_per_launch, const ohm_newton_params *params, int32_t use_graph,
+                             double *waveforms_host, ohm_transient_info *info);
+
 /* ---------------------------------------------------------------- batches --
  * Many independent nonlinear circuits solved by one launch (Monte Carlo
  * corners, parameter sweeps).  No counterpart in the reference, which runs

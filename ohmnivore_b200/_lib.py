@@ -27,6 +27,22 @@ class KrylovParams(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class TransientInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("steps_done", C.c_int32), ("failed_step", C.c_int32),
+                ("krylov_code", C.c_int32), ("newton_iterations", C.c_int64), ("krylov_iterations", C.c_int64),
+                ("fp64_fallbacks", C.c_int32), ("launches", C.c_int32), ("graph", C.c_int32),
+                ("reserved", C.c_int32), ("max_residual", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# ohm_source (include/ohm.h), 104 bytes
+SOURCE_DTYPE = np.dtype([("kind", "<i4"), ("n_rows", "<i4"), ("rows", "<u4", (2,)), ("sign", "<f8", (2,)),
+                         ("dc", "<f8"), ("p", "<f8", (7,)), ("pwl_offset", "<i4"), ("pwl_count", "<i4")],
+                        align=True)
+
+
 class NewtonParamsC(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
                 ("krylov", KrylovParams), ("initial_guess", C.POINTER(C.c_double)),
@@ -94,6 +110,11 @@ SIGNATURES = {
     "ohm_batch_create": (C.c_int, [_vp, _i64, _vp, _vp, _u32p, _u32p, _dp, _dp, _vp, _vp, _vp, _vp, _dp,
                                    _vp, _vp, _vp, C.POINTER(_vp)]),
     "ohm_batch_destroy": (C.c_int, [_vp]),
+    "ohm_transient_create": (C.c_int, [_vp, _i64, _u32p, _u32p, _dp, _vp, C.c_int32, _dp, C.c_int32, _u32p,
+                                       C.c_int32, C.POINTER(_vp)]),
+    "ohm_transient_destroy": (C.c_int, [_vp]),
+    "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                    C.POINTER(NewtonParamsC), C.c_int32, _dp, C.POINTER(TransientInfo)]),
     "ohm_batch_autotune": (C.c_int, [_vp, C.POINTER(NewtonParamsC), C.c_int32, C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "ohm_batch_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),

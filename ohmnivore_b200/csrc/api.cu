@@ -494,6 +494,14 @@ struct ohm_plan {
     uint32_t *rrow = nullptr, *rrow_ptr = nullptr, *rrow_ids = nullptr;
     unsigned long long *node_scale = nullptr;
     uint8_t *stampflag = nullptr;      // per row: diagonal / rhs written by the stamp map
+    // long rows and long stamp segments (team-cooperative)
+    int n_long = 0, n_long_chunks = 0, n_lseg = 0, n_lseg_chunks = 0;
+    uint8_t *longflag = nullptr, *lseg_flag = nullptr;
+    uint32_t *long_row = nullptr, *long_chunk_ptr = nullptr, *long_chunk_owner = nullptr, *long_chunk_beg = nullptr,
+             *long_chunk_end = nullptr;
+    uint32_t *lseg = nullptr, *lseg_chunk_ptr = nullptr, *lseg_chunk_owner = nullptr, *lseg_chunk_beg = nullptr,
+             *lseg_chunk_end = nullptr;
+    double *long_part = nullptr, *lseg_part = nullptr;
     double *x_good = nullptr;          // DC continuation: last converged point
     double *trace = nullptr;           // kTraceRows x kTraceCols
     Workspace ws;
@@ -515,6 +523,10 @@ static void plan_free(ohm_plan *p) {
     cudaFree(p->rrow); cudaFree(p->rrow_ptr); cudaFree(p->rrow_ids);
     cudaFree(p->node_scale);
     cudaFree(p->stampflag); cudaFree(p->x_good);
+    void *lp[] = {p->longflag, p->lseg_flag, p->long_row, p->long_chunk_ptr, p->long_chunk_owner, p->long_chunk_beg,
+                  p->long_chunk_end, p->lseg, p->lseg_chunk_ptr, p->lseg_chunk_owner, p->lseg_chunk_beg,
+                  p->lseg_chunk_end, p->long_part, p->lseg_part};
+    for (void *q : lp) cudaFree(q);
     cudaFree(p->trace);
     p->ws.release();
     p->isai.release();
@@ -571,6 +583,14 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     p->touched.assign(nnz, 0);
     for (uint32_t sl : ms) p->touched[sl] = 1;
     std::vector<uint8_t> sflag = stamp_flags(size, row_ptrs, col_indices, p->touched, rs);
+    LongSplit lrows, lsegs;
+    split_long(size, row_ptrs, kLongRowMin, kLongRowChunk, 0, lrows);
+    split_long((int64_t)ms.size(), mptr.data(), kLongSegMin, kLongSegChunk, 0, lsegs);
+    split_long((int64_t)rs.size(), rptr.data(), kLongSegMin, kLongSegChunk, (int64_t)ms.size(), lsegs);
+    p->n_long = (int)lrows.item.size();
+    p->n_long_chunks = (int)lrows.chunk_beg.size();
+    p->n_lseg = (int)lsegs.item.size();
+    p->n_lseg_chunks = (int)lsegs.chunk_beg.size();
     p->h_rp.assign(row_ptrs, row_ptrs + size + 1);
     p->h_col.assign(col_indices, col_indices + nnz);
     build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, true, p->pc_pairs);
@@ -600,6 +620,24 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     if (e == cudaSuccess) e = dalloc(&p->node_scale, size);
     if (e == cudaSuccess) e = up(&p->stampflag, sflag.data(), size, s);
     if (e == cudaSuccess) e = dalloc(&p->x_good, size);
+    if (e == cudaSuccess && p->n_long) {
+        e = up(&p->longflag, lrows.flag.data(), lrows.flag.size(), s);
+        if (e == cudaSuccess) e = up(&p->long_row, lrows.item.data(), lrows.item.size(), s);
+        if (e == cudaSuccess) e = up(&p->long_chunk_ptr, lrows.chunk_ptr.data(), lrows.chunk_ptr.size(), s);
+        if (e == cudaSuccess) e = up(&p->long_chunk_owner, lrows.chunk_owner.data(), lrows.chunk_owner.size(), s);
+        if (e == cudaSuccess) e = up(&p->long_chunk_beg, lrows.chunk_beg.data(), lrows.chunk_beg.size(), s);
+        if (e == cudaSuccess) e = up(&p->long_chunk_end, lrows.chunk_end.data(), lrows.chunk_end.size(), s);
+        if (e == cudaSuccess) e = dalloc(&p->long_part, lrows.chunk_beg.size());
+    }
+    if (e == cudaSuccess && p->n_lseg) {
+        e = up(&p->lseg_flag, lsegs.flag.data(), lsegs.flag.size(), s);
+        if (e == cudaSuccess) e = up(&p->lseg, lsegs.item.data(), lsegs.item.size(), s);
+        if (e == cudaSuccess) e = up(&p->lseg_chunk_ptr, lsegs.chunk_ptr.data(), lsegs.chunk_ptr.size(), s);
+        if (e == cudaSuccess) e = up(&p->lseg_chunk_owner, lsegs.chunk_owner.data(), lsegs.chunk_owner.size(), s);
+        if (e == cudaSuccess) e = up(&p->lseg_chunk_beg, lsegs.chunk_beg.data(), lsegs.chunk_beg.size(), s);
+        if (e == cudaSuccess) e = up(&p->lseg_chunk_end, lsegs.chunk_end.data(), lsegs.chunk_end.size(), s);
+        if (e == cudaSuccess) e = dalloc(&p->lseg_part, lsegs.chunk_beg.size());
+    }
     if (e == cudaSuccess) e = dalloc(&p->trace, (size_t)kTraceRows * kTraceCols);
     if (e == cudaSuccess) e = p->ws.alloc(size, c->num_sms);
     if (e == cudaSuccess && nnz) {
@@ -707,6 +745,12 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.n_nodes = (int)std::min<int64_t>(np->n_nodes, p->n);
     a.stampflag = p->stampflag;
     a.x_good = p->x_good;
+    a.n_long = p->n_long; a.n_long_chunks = p->n_long_chunks; a.longflag = p->longflag;
+    a.long_row = p->long_row; a.long_chunk_ptr = p->long_chunk_ptr; a.long_chunk_owner = p->long_chunk_owner;
+    a.long_chunk_beg = p->long_chunk_beg; a.long_chunk_end = p->long_chunk_end; a.long_part = p->long_part;
+    a.n_lseg = p->n_lseg; a.n_lseg_chunks = p->n_lseg_chunks; a.lseg_flag = p->lseg_flag; a.lseg = p->lseg;
+    a.lseg_chunk_ptr = p->lseg_chunk_ptr; a.lseg_chunk_owner = p->lseg_chunk_owner;
+    a.lseg_chunk_beg = p->lseg_chunk_beg; a.lseg_chunk_end = p->lseg_chunk_end; a.lseg_part = p->lseg_part;
     return OHM_OK;
 }
 
@@ -719,6 +763,19 @@ static ohm_status check_newton(const ohm_newton_params *np) {
         return fail(OHM_ERR_INVALID_ARG, "continuation needs n_nodes (the node rows of the MNA system)");
     return ohm_check_krylov(&np->krylov);
 }
+
+ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, KernelArgs &a,
+                                int64_t *nnz) {
+    if (!p) return fail(OHM_ERR_INVALID_ARG, "plan is null");
+    ohm_status st = check_newton(np);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaSetDevice(p->ctx->device));
+    st = plan_args(p, np, x_dev, a);
+    if (nnz) *nnz = p->nnz;
+    return st;
+}
+
+ohm_ctx *ohm_plan_context(ohm_plan *p) { return p ? p->ctx : nullptr; }
 
 extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const ohm_newton_params *np,
                                              ohm_solve_info *info) {

@@ -158,4 +158,37 @@ inline std::vector<uint8_t> stamp_flags(int64_t n, const uint32_t *rp, const uin
     return f;
 }
 
+// Items whose range ptr[i]..ptr[i+1] is longer than min_len, each cut into
+// consecutive chunks of at most `chunk` entries (long rows of a CSR matrix,
+// stamp-map entries with many contributions).
+struct LongSplit {
+    std::vector<uint32_t> item, chunk_ptr, chunk_owner, chunk_beg, chunk_end;
+    std::vector<uint8_t> flag;      // per item index: 1 if long
+};
+
+inline void split_long(int64_t count, const uint32_t *ptr, uint32_t min_len, uint32_t chunk, int64_t item_offset,
+                       LongSplit &out) {
+    if (out.chunk_ptr.empty()) out.chunk_ptr.push_back(0);
+    for (int64_t i = 0; i < count; ++i) {
+        const uint32_t b = ptr[i], e = ptr[i + 1];
+        const bool long_item = e - b > min_len;
+        out.flag.push_back(long_item ? 1 : 0);
+        if (!long_item) continue;
+        const uint32_t owner = (uint32_t)out.item.size();
+        out.item.push_back((uint32_t)(i + item_offset));
+        for (uint32_t c = b; c < e; c += chunk) {
+            out.chunk_owner.push_back(owner);
+            out.chunk_beg.push_back(c);
+            out.chunk_end.push_back(std::min(e, c + chunk));
+        }
+        out.chunk_ptr.push_back((uint32_t)out.chunk_beg.size());
+    }
+}
+
+// Thresholds: rows with more nonzeros than kLongRowMin, and stamp-map
+// entries with more contributions than kLongSegMin, are handled by the whole
+// team in chunks.
+constexpr uint32_t kLongRowMin = 4096, kLongRowChunk = 1024;
+constexpr uint32_t kLongSegMin = 256, kLongSegChunk = 256;
+
 }  // namespace ohm

@@ -50,6 +50,11 @@ struct LaunchTarget {
 ohm_status ohm_launch_persistent(const LaunchTarget &t, ohm::KernelArgs &a, int64_t nnz, int *launches);
 ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, int launches);
 ohm_status ohm_check_krylov(const ohm_krylov_params *p);
+// Kernel arguments of a Newton solve on a plan (validated params), its
+// context, and the launch of a plan-sized persistent kernel (api.cu).
+ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, ohm::KernelArgs &a,
+                                int64_t *nnz);
+ohm_ctx *ohm_plan_context(ohm_plan *p);
 cudaError_t ohm_f64_to_f32(const double *in, float *out, int64_t n, cudaStream_t s);
 
 // Child-object bookkeeping (see ohm_ctx::live_objects).

@@ -126,6 +126,18 @@ struct KernelArgs {
     const uint32_t *rrow, *rrow_ptr, *rrow_ids;
     unsigned long long *node_scale;
 
+    // Long rows / long stamp segments handled by the whole team (see
+    // spmv_long and the stamp pass).  longflag[i] = 1 for a long row.
+    int n_long, n_long_chunks;
+    const uint8_t *longflag;
+    const uint32_t *long_row, *long_chunk_ptr, *long_chunk_owner, *long_chunk_beg, *long_chunk_end;
+    double *long_part;
+    // stamp segments (index k over mslots then rrows) with many contributions
+    int n_lseg, n_lseg_chunks;
+    const uint32_t *lseg, *lseg_chunk_ptr, *lseg_chunk_owner, *lseg_chunk_beg, *lseg_chunk_end;
+    const uint8_t *lseg_flag;    // per mslot/rrow entry: 1 if handled as a long segment
+    double *lseg_part;
+
     // DC continuation (src/analysis/dc.rs): 1 = on failure of the direct
     // Newton solve, run source stepping (MOSFET circuits), GMIN stepping and
     // pseudo-transient continuation on the device.  n_nodes: node rows come
@@ -243,7 +255,7 @@ template <int LPR, typename Acc, typename TA, typename X, typename F>
 __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
                                           const uint32_t *__restrict__ col,
                                           const TA *__restrict__ val, const uint8_t *rowflag,
-                                          int r0, int r1, X x, F f) {
+                                          int r0, int r1, X x, F f, const uint8_t *skip = nullptr) {
     constexpr int U = kRowsInFlight;
     const int lane = threadIdx.x % LPR;
     const int group = threadIdx.x / LPR;
@@ -257,7 +269,7 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             row[u] = tile + group + u * ngroups;
-            const bool ok = row[u] < r1;
+            const bool ok = row[u] < r1 && !(skip != nullptr && skip[row[u]] != 0);
             beg[u] = ok ? rp[row[u]] : 0u;
             end[u] = ok ? rp[row[u] + 1] : 0u;
             slow[u] = ok && rowflag != nullptr && rowflag[row[u]] != 0;
@@ -283,8 +295,41 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (lane == 0 && row[u] < r1) f(row[u], (double)acc[u]);
+            if (lane == 0 && row[u] < r1 && !(skip != nullptr && skip[row[u]] != 0)) f(row[u], (double)acc[u]);
     }
+}
+
+// Long rows (a hub node such as a supply rail, whose row holds a nonzero per
+// connected device) are skipped by spmv_rows and computed by the whole team:
+// one warp per chunk of at most a few hundred nonzeros writes a partial, a
+// team sync, then one warp per long row sums its partials in a fixed order
+// and calls f(row, y) like spmv_rows does.  Returns false if the sync gave up.
+template <typename Acc, class Team, typename TA, typename X, typename F>
+__device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const uint32_t *__restrict__ col,
+                                          const TA *__restrict__ val, const uint8_t *rowflag, X x, F f) {
+    if (a.n_long == 0) return true;
+    const int lane = threadIdx.x & 31;
+    const int warp = g.gtid >> 5, nwarps = g.gstride >> 5;
+    for (int c = warp; c < a.n_long_chunks; c += nwarps) {
+        const uint32_t row = a.long_row[a.long_chunk_owner[c]];
+        const bool slow = rowflag != nullptr && rowflag[row] != 0;
+        Acc acc = Acc(0);
+        for (uint32_t k = a.long_chunk_beg[c] + lane; k < a.long_chunk_end[c]; k += 32)
+            acc += (Acc)val[k] * (Acc)x((int)col[k], slow);
+        double s = (double)acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) a.long_part[c] = s;
+    }
+    if (!g.sync()) return false;
+    for (int j = warp; j < a.n_long; j += nwarps) {
+        double s = 0.0;
+        for (uint32_t c = a.long_chunk_ptr[j] + lane; c < a.long_chunk_ptr[j + 1]; c += 32) s += a.long_part[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) f((int)a.long_row[j], s);
+    }
+    return true;
 }
 
 // Per-row Krylov record: p, v, r and the preconditioner's self coefficient.
@@ -429,7 +474,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 return cvt<T>(z);
             };
             double acc1[2] = {0.0, 0.0};
-            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, phat_at, [&](int i, double y) {
+            auto ab_row = [&](int i, double y) {
                 const KRec<T> q = cur[i];
                 KRec<T> o;
                 o.p = pnew(q);
@@ -440,7 +485,9 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 phat[i] = phat_at(i, true);
                 acc1[0] += (double)rhat[i] * (double)o.v;
                 acc1[1] += (double)o.v * (double)o.v;
-            });
+            };
+            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, phat_at, ab_row, a.longflag);
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row)) return kKrylovAbort;
             {
                 if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
             }
@@ -468,7 +515,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 return cvt<T>(z);
             };
             double acc3[4] = {0.0, 0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t), ||W s||^2
-            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, shat_at, [&](int i, double y) {
+            auto cd_row = [&](int i, double y) {
                 const T si = s_of(nxt[i]);
                 const T ti = cvt<T>(y);
                 s[i] = si;
@@ -479,7 +526,9 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 acc3[1] += (double)ti * (double)si;
                 acc3[2] += (double)ti * (double)ti;
                 acc3[3] += ws * ws;
-            });
+            };
+            spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, shat_at, cd_row, a.longflag);
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row)) return kKrylovAbort;
             {
                 if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
             }
@@ -593,8 +642,43 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
                 }
             }
             OHM_SYNC_OR(false);
-            // stamp map: each touched slot / row = base + contributions in canonical order
+            // stamp map: each touched slot / row = base + contributions in canonical order;
+            // entries with many contributions are summed by warps in chunks first
+            if (a.n_lseg) {
+                const int lane = threadIdx.x & 31;
+                for (int c = gtid >> 5; c < a.n_lseg_chunks; c += gstride >> 5) {
+                    const bool mat = (int)a.lseg[a.lseg_chunk_owner[c]] < a.n_mslots;
+                    const uint32_t *ids = mat ? a.mslot_ids : a.rrow_ids;
+                    const double *src = mat ? a.mstamp : a.rstamp;
+                    double acc = 0.0;
+                    for (uint32_t j = a.lseg_chunk_beg[c] + lane; j < a.lseg_chunk_end[c]; j += 32) acc += src[ids[j]];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                    if (lane == 0) a.lseg_part[c] = acc;
+                }
+                OHM_SYNC_OR(false);
+                for (int q = gtid >> 5; q < a.n_lseg; q += gstride >> 5) {
+                    double acc = 0.0;
+                    for (uint32_t c = a.lseg_chunk_ptr[q] + lane; c < a.lseg_chunk_ptr[q + 1]; c += 32)
+                        acc += a.lseg_part[c];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                    if (lane == 0) {
+                        const int k = (int)a.lseg[q];
+                        if (k < a.n_mslots) {
+                            const uint32_t slot = a.mslot[k];
+                            const double v = a.base_vals[slot] + acc;
+                            a.vals64[slot] = v;
+                            if (a.vals32) a.vals32[slot] = (float)v;
+                        } else {
+                            const uint32_t row = a.rrow[k - a.n_mslots];
+                            a.b[row] = cfg.src * a.base_b[row] + acc;
+                        }
+                    }
+                }
+            }
             for (int k = gtid; k < a.n_mslots + a.n_rrows; k += gstride) {
+                if (a.lseg_flag != nullptr && a.lseg_flag[k]) continue;
                 if (k < a.n_mslots) {
                     const uint32_t slot = a.mslot[k];
                     double acc = a.base_vals[slot];
@@ -637,8 +721,7 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         const double *xv = a.x;
         auto x_at = [&](int j, bool) -> double { return xv[j]; };
-        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at,
-                               [&](int i, double ax) {
+        auto res_row = [&](int i, double ax) {
             const double bi = a.b[i];
             const double ri = bi - ax;
             a.r64[i] = ri;
@@ -651,7 +734,10 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
                 acc[2] += (wi * bi) * (wi * bi);
                 acc[3] += (wi * ri) * (wi * ri);
             }
-        });
+        };
+        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at, res_row,
+                               a.longflag);
+        if (!spmv_long<double>(a, g, a.col, a.vals64, (const uint8_t *)nullptr, x_at, res_row)) return false;
         {
             if (!g.template allreduce<4>(acc)) return false;
         }
@@ -781,11 +867,13 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
         double acc[1] = {0.0};
         const double *xv = a.x;
         auto x_at = [&](int j, bool) -> double { return xv[j]; };
-        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at,
-                               [&](int i, double ax) {
+        auto fin_row = [&](int i, double ax) {
             const double ri = a.b[i] - ax;
             acc[0] += ri * ri;
-        });
+        };
+        spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at, fin_row,
+                               a.longflag);
+        if (!spmv_long<double>(a, g, a.col, a.vals64, (const uint8_t *)nullptr, x_at, fin_row)) return false;
         if (!g.template allreduce<1>(acc)) return false;
         final_res = sqrt(acc[0]);
         if (a.require_true_residual && !(final_res < a.krylov_tol * bnorm_last)) {

@@ -1,0 +1,461 @@
+// Fixed-step backward-Euler transient with a Newton solve per step.
+//
+// One persistent cooperative kernel runs a chunk of steps; per step the grid
+//   1. forms the BE right-hand side b_n = b(t_n) + (C/h) x_{n-1}
+//      (transient.rs:326-333) with the sources evaluated on the device
+//      (transient_source.rs:8-118), C in its own compact CSR,
+//   2. runs the Newton loop (newton_run) on the companion system whose base
+//      values A = G + C/h were formed once for the run (transient.rs:285-323),
+//      starting from x_{n-1},
+//   3. records the probe rows of x_n.
+// The host launches ceil(n_steps / steps_per_launch) chunks, optionally
+// recorded once as a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "host_util.h"
+
+using namespace ohm;
+
+namespace {
+
+// Device-side run record, accumulated by the grid leader.
+struct TranDev {
+    int status, steps_done, failed_step, kcode;
+    long long newton_its, krylov_its;
+    int fallbacks, pad;
+    double max_residual;
+};
+
+struct TranArgs {
+    int s0, s1;                        // steps [s0, s1) of this launch
+    double t0, h;
+    const uint32_t *c_rp, *c_col;
+    const double *c_val;
+    const int32_t *src_of_row;         // per row: index into srow_ptr, -1 none
+    const uint32_t *srow_ptr, *srow_src;
+    const double *srow_sign;
+    const ohm_source *src;
+    const double *pwl;
+    const uint32_t *probe;
+    int n_probes;
+    double *wave;                      // n_steps x n_probes
+    double *beff;                      // base rhs of the current step
+    TranDev *st;
+};
+
+// Source waveforms, the formulas of transient_source.rs:39-118.
+__device__ double source_value(const ohm_source &s, double t, const double *pwl) {
+    const double *p = s.p;
+    switch (s.kind) {
+        case OHM_TRAN_PULSE: {
+            const double v1 = p[0], v2 = p[1], td = p[2], tr = p[3], tf = p[4], pw = p[5], per = p[6];
+            if (t < td) return v1;
+            const double trel = (per > 0.0 && per < 1.7976931348623157e308) ? fmod(t - td, per) : t - td;
+            if (trel < tr) return tr > 0.0 ? v1 + (v2 - v1) * trel / tr : v2;
+            if (trel < tr + pw) return v2;
+            if (trel < tr + pw + tf) return tf > 0.0 ? v2 + (v1 - v2) * (trel - tr - pw) / tf : v1;
+            return v1;
+        }
+        case OHM_TRAN_SIN: {
+            const double vo = p[0], va = p[1], freq = p[2], td = p[3], theta = p[4];
+            if (t < td) return vo;
+            const double dt = t - td;
+            const double env = theta != 0.0 ? exp(-dt * theta) : 1.0;
+            return vo + va * sin(2.0 * 3.14159265358979323846 * freq * dt) * env;
+        }
+        case OHM_TRAN_PWL: {
+            const double *q = pwl + 2 * (size_t)s.pwl_offset;
+            const int m = s.pwl_count;
+            if (m <= 0) return 0.0;
+            if (t <= q[0]) return q[1];
+            if (t >= q[2 * (m - 1)]) return q[2 * (m - 1) + 1];
+            for (int i = 1; i < m; ++i) {
+                if (t <= q[2 * i]) {
+                    const double t0 = q[2 * (i - 1)], v0 = q[2 * (i - 1) + 1], t1 = q[2 * i], v1 = q[2 * i + 1];
+                    return v0 + (v1 - v0) * ((t - t0) / (t1 - t0));
+                }
+            }
+            return q[2 * (m - 1) + 1];
+        }
+        case OHM_TRAN_EXP: {
+            const double v1 = p[0], v2 = p[1], td1 = p[2], tau1 = p[3], td2 = p[4], tau2 = p[5];
+            if (t < td1) return v1;
+            const double rise = (v2 - v1) * (1.0 - exp(-(t - td1) / tau1));
+            if (t < td2) return v1 + rise;
+            const double fall = (v1 - v2) * (1.0 - exp(-(t - td2) / tau2));
+            return v1 + rise + fall;
+        }
+        default:
+            return s.dc;
+    }
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a, TranArgs T) {
+    __shared__ double smem[32 * 4];
+    GridTeam g;
+    g.G = gridDim.x;
+    g.bid = blockIdx.x;
+    g.r0 = (int)(((long long)a.n * g.bid) / g.G);
+    g.r1 = (int)(((long long)a.n * (g.bid + 1)) / g.G);
+    g.gtid = g.bid * blockDim.x + threadIdx.x;
+    g.gstride = g.G * blockDim.x;
+    g.smem = smem;
+    g.partials = a.partials;
+    g.red = 0;
+    g.epoch = 0;
+    g.gs = a.gs;
+    if (T.st->status != 0) return;     // an earlier chunk failed (uniform: written before this launch)
+    const double inv_h = 1.0 / T.h;
+    for (int s = T.s0; s < T.s1; ++s) {
+        const double tn = T.t0 + (double)(s + 1) * T.h;
+        // ---- b_n = b(t_n) + (C/h) x_{n-1} for the rows of this block ----
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += blockDim.x) {
+            double bs = 0.0;
+            const int q = T.src_of_row[i];
+            if (q >= 0)
+                for (uint32_t e = T.srow_ptr[q]; e < T.srow_ptr[q + 1]; ++e)
+                    bs += T.srow_sign[e] * source_value(T.src[T.srow_src[e]], tn, T.pwl);
+            double cx = 0.0;
+            for (uint32_t k = T.c_rp[i]; k < T.c_rp[i + 1]; ++k) cx += T.c_val[k] * a.x[T.c_col[k]];
+            const double bb = bs + cx * inv_h;
+            T.beff[i] = bb;
+            a.b[i] = bb;
+        }
+        if (!g.sync()) return;
+        // ---- Newton on the companion system, from x_{n-1} ----
+        RunOut o;
+        RunCfg c{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+        if (!newton_run<LPR>(a, g, c, o)) return;
+        if (g.leader()) {
+            TranDev &d = *T.st;
+            d.newton_its += o.outer_done;
+            d.krylov_its += o.kiters;
+            d.fallbacks += o.fallbacks;
+            d.kcode = o.kcode;
+            if (o.status == kOk) {
+                d.steps_done = s + 1;
+            } else {
+                d.status = o.status;
+                d.failed_step = s;
+                d.max_residual = o.last_dmax;
+            }
+        }
+        if (o.status != kOk) return;
+        for (int k = g.gtid; k < T.n_probes; k += g.gstride)
+            T.wave[(size_t)s * T.n_probes + k] = a.x[T.probe[k]];
+    }
+}
+
+using TranFn = void (*)(KernelArgs, TranArgs);
+
+TranFn pick_tran(int lpr) {
+    switch (lpr) {
+        case 1: return transient_kernel<1>;
+        case 2: return transient_kernel<2>;
+        case 4: return transient_kernel<4>;
+        default: return transient_kernel<8>;
+    }
+}
+
+// A = G + C/h on the plan's pattern, copied to the assembled arrays.
+__global__ void companion_kernel(const double *G, double *A, double *vals64, float *vals32, int64_t nnz,
+                                 const uint32_t *c_slot, const double *c_val, int64_t c_nnz, double inv_h,
+                                 int phase) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (phase == 0) {
+        for (int64_t k = i0; k < nnz; k += stride) A[k] = G[k];
+    } else if (phase == 1) {
+        for (int64_t k = i0; k < c_nnz; k += stride) A[c_slot[k]] += c_val[k] * inv_h;   // C slots are distinct
+    } else {
+        for (int64_t k = i0; k < nnz; k += stride) {
+            vals64[k] = A[k];
+            if (vals32) vals32[k] = (float)A[k];
+        }
+    }
+}
+
+__global__ void restore_kernel(const double *G, double *vals64, float *vals32, int64_t nnz) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) {
+        vals64[k] = G[k];
+        if (vals32) vals32[k] = (float)G[k];
+    }
+}
+
+int steps_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096)); }
+
+int tran_lpr(int64_t n, int64_t nnz) {
+    const double avg = n > 0 ? (double)nnz / (double)n : 1.0;
+    return avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : 8));
+}
+
+}  // namespace
+
+struct ohm_transient {
+    ohm_plan *plan = nullptr;
+    ohm_ctx *ctx = nullptr;
+    int64_t n = 0, c_nnz = 0, nnz = 0;
+    int n_probes = 0;
+    std::vector<void *> allocs;
+    uint32_t *c_rp = nullptr, *c_col = nullptr, *c_slot = nullptr;
+    double *c_val = nullptr, *aval = nullptr, *beff = nullptr, *pwl = nullptr;
+    int32_t *src_of_row = nullptr;
+    uint32_t *srow_ptr = nullptr, *srow_src = nullptr, *probe = nullptr;
+    double *srow_sign = nullptr;
+    ohm_source *src = nullptr;
+    TranDev *st = nullptr;
+    double *wave = nullptr;
+    int64_t wave_cap = 0;
+
+    template <typename T>
+    cudaError_t put(T **dst, const T *h, size_t count) {
+        cudaError_t e = dalloc(dst, count);
+        if (e == cudaSuccess) allocs.push_back((void *)*dst);
+        if (e == cudaSuccess && h && count)
+            e = cudaMemcpyAsync(*dst, h, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+        return e;
+    }
+};
+
+extern "C" ohm_status ohm_transient_create(ohm_plan *plan, int64_t c_nnz, const uint32_t *c_row_ptr,
+                                           const uint32_t *c_col, const double *c_values, const ohm_source *sources,
+                                           int32_t n_sources, const double *pwl_points, int32_t n_pwl_points,
+                                           const uint32_t *probe_rows, int32_t n_probes, ohm_transient **out) {
+    if (!plan || !out || !c_row_ptr || c_nnz < 0 || n_sources < 0 || n_probes < 0 || n_pwl_points < 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "bad transient arguments");
+    *out = nullptr;
+    if ((c_nnz && (!c_col || !c_values)) || (n_sources && !sources) || (n_probes && !probe_rows) ||
+        (n_pwl_points && !pwl_points))
+        return ohm_fail(OHM_ERR_INVALID_ARG, "null array");
+    ohm_ctx *c = ohm_plan_context(plan);
+    ohm_newton_params np;
+    ohm_newton_params_default(&np);
+    KernelArgs a;
+    int64_t nnz = 0;
+    ohm_status st = ohm_plan_kernel_args(plan, &np, nullptr, a, &nnz);
+    if (st != OHM_OK) return st;
+    const int64_t n = a.n;
+    st = check_csr(n, c_nnz, c_row_ptr, c_col);
+    if (st != OHM_OK) return ohm_fail(st, "capacitance matrix: %s", ohm_last_error());
+    // host copy of the plan pattern to locate each C entry's slot
+    std::vector<uint32_t> rp(n + 1), col(nnz);
+    CUDA_TRY(cudaMemcpy(rp.data(), a.row_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (nnz) CUDA_TRY(cudaMemcpy(col.data(), a.col, nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> slot(c_nnz);
+    for (int64_t i = 0; i < n; ++i) {
+        for (uint32_t k = c_row_ptr[i]; k < c_row_ptr[i + 1]; ++k) {
+            const auto b = col.begin() + rp[i], e = col.begin() + rp[i + 1];
+            const auto it = std::lower_bound(b, e, c_col[k]);
+            if (it == e || *it != c_col[k])
+                return ohm_fail(OHM_ERR_COMPILE, "capacitance entry (%lld, %u) is not on the conductance pattern",
+                                (long long)i, c_col[k]);
+            slot[k] = (uint32_t)(it - col.begin());
+        }
+    }
+    // sources per rhs row, in source order
+    std::vector<std::vector<std::pair<uint32_t, double>>> per_row(n);
+    for (int32_t k = 0; k < n_sources; ++k) {
+        const ohm_source &s = sources[k];
+        if (s.n_rows < 0 || s.n_rows > 2) return ohm_fail(OHM_ERR_INVALID_ARG, "source %d: n_rows must be 0-2", k);
+        if (s.kind < OHM_TRAN_DC || s.kind > OHM_TRAN_EXP)
+            return ohm_fail(OHM_ERR_INVALID_ARG, "source %d: unknown kind %d", k, s.kind);
+        if (s.kind == OHM_TRAN_PWL && (s.pwl_offset < 0 || s.pwl_count < 0 ||
+                                       (int64_t)s.pwl_offset + s.pwl_count > n_pwl_points))
+            return ohm_fail(OHM_ERR_INVALID_ARG, "source %d: PWL points out of range", k);
+        for (int j = 0; j < s.n_rows; ++j) {
+            if ((int64_t)s.rows[j] >= n) return ohm_fail(OHM_ERR_INVALID_ARG, "source %d: row out of range", k);
+            per_row[s.rows[j]].push_back({(uint32_t)k, s.sign[j]});
+        }
+    }
+    std::vector<int32_t> src_of_row(n, -1);
+    std::vector<uint32_t> srow_ptr(1, 0), srow_src;
+    std::vector<double> srow_sign;
+    for (int64_t i = 0; i < n; ++i) {
+        if (per_row[i].empty()) continue;
+        src_of_row[i] = (int32_t)(srow_ptr.size() - 1);
+        for (auto &pr : per_row[i]) { srow_src.push_back(pr.first); srow_sign.push_back(pr.second); }
+        srow_ptr.push_back((uint32_t)srow_src.size());
+    }
+    for (int32_t k = 0; k < n_probes; ++k)
+        if ((int64_t)probe_rows[k] >= n) return ohm_fail(OHM_ERR_INVALID_ARG, "probe %d out of range", k);
+
+    ohm_transient *t = new ohm_transient();
+    t->plan = plan; t->ctx = c; t->n = n; t->c_nnz = c_nnz; t->nnz = nnz; t->n_probes = n_probes;
+    cudaError_t e = t->put(&t->c_rp, c_row_ptr, n + 1);
+    if (e == cudaSuccess) e = t->put(&t->c_col, c_col, c_nnz);
+    if (e == cudaSuccess) e = t->put(&t->c_val, c_values, c_nnz);
+    if (e == cudaSuccess) e = t->put(&t->c_slot, slot.data(), c_nnz);
+    if (e == cudaSuccess) e = t->put(&t->aval, (const double *)nullptr, nnz);
+    if (e == cudaSuccess) e = t->put(&t->beff, (const double *)nullptr, n);
+    if (e == cudaSuccess) e = t->put(&t->pwl, pwl_points, 2 * (size_t)n_pwl_points);
+    if (e == cudaSuccess) e = t->put(&t->src_of_row, src_of_row.data(), n);
+    if (e == cudaSuccess) e = t->put(&t->srow_ptr, srow_ptr.data(), srow_ptr.size());
+    if (e == cudaSuccess) e = t->put(&t->srow_src, srow_src.data(), srow_src.size());
+    if (e == cudaSuccess) e = t->put(&t->srow_sign, srow_sign.data(), srow_sign.size());
+    if (e == cudaSuccess) e = t->put(&t->src, sources, n_sources);
+    if (e == cudaSuccess) e = t->put(&t->probe, probe_rows, n_probes);
+    if (e == cudaSuccess) e = t->put(&t->st, (const TranDev *)nullptr, 1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        for (void *q : t->allocs) cudaFree(q);
+        delete t;
+        return ohm_fail(OHM_ERR_CUDA, "transient upload: %s", cudaGetErrorString(e));
+    }
+    ohm_ctx_retain(c);
+    *out = t;
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_transient_destroy(ohm_transient *t) {
+    if (!t) return OHM_OK;
+    ohm_ctx *c = t->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (void *q : t->allocs) cudaFree(q);
+    cudaFree(t->wave);
+    delete t;
+    ohm_ctx_release(c);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double t0, double h, int32_t n_steps,
+                                        int32_t steps_per_launch, const ohm_newton_params *np, int32_t use_graph,
+                                        double *waveforms_host, ohm_transient_info *info) {
+    if (!t || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (!(h > 0.0) || n_steps < 0 || steps_per_launch <= 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 0, steps_per_launch > 0");
+    if (np->continuation) return ohm_fail(OHM_ERR_INVALID_ARG, "continuation is for DC solves, not transient steps");
+    if (np->krylov.precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi");
+    ohm_ctx *c = t->ctx;
+    KernelArgs a;
+    int64_t nnz = 0;
+    ohm_status st = ohm_plan_kernel_args(t->plan, np, x_dev, a, &nnz);
+    if (st != OHM_OK) return st;
+    if (np->initial_guess)
+        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int64_t need = (int64_t)n_steps * t->n_probes;
+    if (need > t->wave_cap) {
+        cudaFree(t->wave);
+        t->wave = nullptr;
+        t->wave_cap = 0;
+        CUDA_TRY(dalloc(&t->wave, (size_t)need));
+        t->wave_cap = need;
+    }
+    // companion base A = G + C/h, assembled arrays start from it
+    const double *G = a.base_vals;
+    for (int phase = 0; phase < 3; ++phase) {
+        companion_kernel<<<steps_grid(phase == 1 ? t->c_nnz : nnz), 256, 0, c->stream>>>(
+            G, t->aval, a.vals64, a.vals32, nnz, t->c_slot, t->c_val, t->c_nnz, 1.0 / h, phase);
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaMemsetAsync(t->st, 0, sizeof(TranDev), c->stream));
+    a.base_vals = t->aval;
+    a.base_b = t->beff;
+    a.trace = nullptr;
+    a.continuation = 0;
+
+    TranArgs T{};
+    T.t0 = t0; T.h = h;
+    T.c_rp = t->c_rp; T.c_col = t->c_col; T.c_val = t->c_val;
+    T.src_of_row = t->src_of_row; T.srow_ptr = t->srow_ptr; T.srow_src = t->srow_src; T.srow_sign = t->srow_sign;
+    T.src = t->src; T.pwl = t->pwl; T.probe = t->probe; T.n_probes = t->n_probes; T.wave = t->wave;
+    T.beff = t->beff; T.st = t->st;
+
+    // grid: as for the persistent Newton solver
+    TranFn fn = pick_tran(tran_lpr(t->n, nnz));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0));
+    if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "transient kernel does not fit on an SM");
+    per_sm = std::min(per_sm, 2);
+    int64_t want = (t->n + kSolverBlock - 1) / kSolverBlock;
+    want = std::max<int64_t>(want, ((int64_t)a.nd + a.nq + a.nm + kSolverBlock - 1) / kSolverBlock);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
+    a.gs.count = (unsigned long long *)c->sync_words;
+    a.gs.error = (int *)(c->sync_words + 2);
+    a.info = c->info_dev;
+
+    const int n_launch = (n_steps + steps_per_launch - 1) / steps_per_launch;
+    auto enqueue = [&]() -> cudaError_t {
+        for (int l = 0; l < n_launch; ++l) {
+            T.s0 = l * steps_per_launch;
+            T.s1 = std::min(n_steps, T.s0 + steps_per_launch);
+            cudaError_t e = cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream);
+            if (e != cudaSuccess) return e;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(kSolverBlock);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = c->stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            e = cudaLaunchKernelEx(&cfg, fn, a, T);
+            if (e != cudaSuccess) return e;
+        }
+        if (waveforms_host && need)
+            return cudaMemcpyAsync(waveforms_host, t->wave, (size_t)need * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream);
+        return cudaSuccess;
+    };
+
+    int graph_used = 0;
+    if (use_graph && n_launch > 0) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue();
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "transient graph: %s", cudaGetErrorString(e));
+        graph_used = 1;
+    } else {
+        cudaError_t e = enqueue();
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "transient launch: %s", cudaGetErrorString(e));
+    }
+    // restore the plan's assembled system to its conductance base
+    restore_kernel<<<steps_grid(nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, nnz);
+    CUDA_TRY(cudaGetLastError());
+    TranDev d{};
+    unsigned int words[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(&d, t->st, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    ohm_status rs = OHM_OK;
+    if (words[2] != 0) {
+        rs = ohm_fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
+    } else if (d.status != 0) {
+        rs = ohm_fail(d.status == kErrSolve ? OHM_ERR_SOLVE
+                      : (d.status == kErrNewtonNumerical ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
+                      "transient step %d at t = %.6e failed (status %d, krylov code %d)", d.failed_step,
+                      t0 + (d.failed_step + 1) * h, d.status, d.kcode);
+    }
+    if (info) {
+        std::memset(info, 0, sizeof *info);
+        info->status = rs;
+        info->steps_done = d.steps_done;
+        info->failed_step = d.status != 0 ? d.failed_step : -1;
+        info->krylov_code = d.kcode;
+        info->newton_iterations = d.newton_its;
+        info->krylov_iterations = d.krylov_its;
+        info->fp64_fallbacks = d.fallbacks;
+        info->launches = n_launch;
+        info->graph = graph_used;
+        info->max_residual = d.max_residual;
+    }
+    return rs;
+}

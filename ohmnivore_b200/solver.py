@@ -447,6 +447,90 @@ class NewtonBatch:
         return [a.as_dict() for a in arr]
 
 
+def pack_sources(sysm):
+    """``ohm_source`` records and PWL points for the sources of an MnaSystem
+    (``collect_source_info``, src/analysis/transient.rs:212-262): a source
+    with a transient function (kind, params) uses it, otherwise its DC value."""
+    srcs = np.zeros(len(sysm.sources), dtype=_lib.SOURCE_DTYPE)
+    pwl = []
+    for k, (_, entries, dc, tran) in enumerate(sysm.sources):
+        rec = srcs[k]
+        rec["n_rows"] = len(entries)
+        for j, (row, sign) in enumerate(entries):
+            rec["rows"][j] = row
+            rec["sign"][j] = sign
+        rec["dc"] = 0.0 if dc is None else dc
+        if tran is None:
+            rec["kind"] = -1
+        else:
+            kind, params = tran
+            rec["kind"] = int(kind)
+            if int(kind) == 2:                       # PWL: (t, v) pairs
+                pts = np.asarray(params, dtype=np.float64).reshape(-1, 2)
+                rec["pwl_offset"] = len(pwl)
+                rec["pwl_count"] = len(pts)
+                pwl.extend(map(tuple, pts))
+            else:
+                p = np.zeros(7)
+                p[: len(params)] = params
+                rec["p"] = p
+    pts = np.ascontiguousarray(np.asarray(pwl, dtype=np.float64).reshape(-1))
+    return srcs, pts
+
+
+class Transient:
+    """Fixed-step backward-Euler transient with a Newton solve per step on a
+    :class:`NewtonPlan` (companion system of src/analysis/transient.rs:285-333
+    plus device evaluation); every step runs on the device."""
+
+    def __init__(self, plan: NewtonPlan, probes=()):
+        self.plan = plan
+        self.ctx = plan.ctx
+        sysm = plan.sysm
+        c = sysm.c
+        rp = np.ascontiguousarray(c.row_ptr, dtype=np.uint32)
+        ci = np.ascontiguousarray(c.col, dtype=np.uint32)
+        cv = np.ascontiguousarray(c.val, dtype=np.float64)
+        self.sources, self.pwl = pack_sources(sysm)
+        self.probes = np.ascontiguousarray(probes, dtype=np.uint32)
+        h = C.c_void_p()
+        st = self.ctx.lib.ohm_transient_create(
+            plan._h, len(cv), u32ptr(rp), u32ptr(ci), dptr(cv) if len(cv) else None, vptr(self.sources),
+            len(self.sources), dptr(self.pwl) if len(self.pwl) else None, len(self.pwl) // 2,
+            u32ptr(self.probes) if len(self.probes) else None, len(self.probes), C.byref(h))
+        if st != _lib.OK:
+            _raise(st)
+        self._h = h
+        self.last_info = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.ohm_transient_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, x_dev_ptr: int, t0: float, h: float, n_steps: int, params: NewtonParams | None = None,
+            steps_per_launch: int = 100, graph: bool = True, check: bool = True):
+        """Advance x (device pointer, x(t0) in, x(t0 + n_steps h) out).
+        Returns the probe waveforms (n_steps x n_probes)."""
+        p, keep = (params or NewtonParams()).to_c()
+        wave = np.zeros((int(n_steps), len(self.probes)))
+        info = _lib.TransientInfo()
+        st = self.ctx.lib.ohm_transient_run(self._h, C.c_void_p(int(x_dev_ptr)), float(t0), float(h), int(n_steps),
+                                            int(steps_per_launch), C.byref(p), 1 if graph else 0,
+                                            dptr(wave) if wave.size else None, C.byref(info))
+        del keep
+        self.last_info = info.as_dict()
+        if st != _lib.OK and check:
+            _raise(st)
+        return wave
+
+
 class DeviceBuffer:
     """``SolverBackend::Buffer``: FP64 device vector."""
 

@@ -329,3 +329,57 @@ def test_isai1_device_variant_exact_when_pattern_is_full():
     L, U, _ = isai_ref.chow_patel_ref(3, rp, ci, v, sweeps=8)
     np.testing.assert_allclose(ML @ L, np.eye(3), atol=1e-12)
     np.testing.assert_allclose(MU @ U, np.eye(3), atol=1e-12)
+
+
+# ---- transient source functions: known answers of src/analysis/transient_source.rs tests ----
+from oracle import transient_ref as tref  # noqa: E402
+
+_SOURCE_CASES = [
+    # (kind, params, t, expected, tol)
+    (tref.PULSE, (0.0, 5.0, 1.0, 0.1, 0.1, 1.0, 3.0), 0.5, 0.0, 1e-12),     # before delay
+    (tref.PULSE, (0.0, 5.0, 0.0, 1.0, 1.0, 2.0, 6.0), 0.5, 2.5, 1e-12),     # during rise
+    (tref.PULSE, (0.0, 5.0, 0.0, 1.0, 1.0, 2.0, 6.0), 2.0, 5.0, 1e-12),     # at peak
+    (tref.PULSE, (0.0, 5.0, 0.0, 1.0, 1.0, 2.0, 6.0), 3.5, 2.5, 1e-12),     # during fall
+    (tref.PULSE, (0.0, 5.0, 0.0, 1.0, 1.0, 2.0, 6.0), 5.0, 0.0, 1e-12),     # between pulses
+    (tref.PULSE, (0.0, 5.0, 0.0, 0.0, 0.0, 1.0, 2.0), 2.5, 5.0, 1e-12),     # period wrap, high
+    (tref.PULSE, (0.0, 5.0, 0.0, 0.0, 0.0, 1.0, 2.0), 3.5, 0.0, 1e-12),     # period wrap, low
+    (tref.SIN, (1.0, 2.0, 1.0, 1.0, 0.0), 0.5, 1.0, 1e-12),                 # before delay
+    (tref.SIN, (0.0, 1.0, 1.0, 0.0, 0.0), 0.25, 1.0, 1e-12),                # quarter period
+    (tref.SIN, (0.0, 1.0, 1.0, 0.0, 0.0), 0.5, 0.0, 1e-12),                 # half period
+    (tref.SIN, (0.0, 1.0, 1.0, 0.0, 1.0), 0.25, math.exp(-0.25), 1e-12),    # damping
+    (tref.SIN, (2.5, 1.0, 1.0, 0.0, 0.0), 0.25, 3.5, 1e-12),                # offset
+    (tref.PWL, ((1.0, 0.0), (2.0, 5.0)), 0.0, 0.0, 1e-12),                  # before first
+    (tref.PWL, ((1.0, 0.0), (2.0, 5.0)), 3.0, 5.0, 1e-12),                  # after last
+    (tref.PWL, ((0.0, 0.0), (1.0, 10.0), (2.0, 10.0), (3.0, 0.0)), 0.5, 5.0, 1e-12),
+    (tref.PWL, ((0.0, 0.0), (1.0, 10.0), (2.0, 10.0), (3.0, 0.0)), 1.5, 10.0, 1e-12),
+    (tref.PWL, ((0.0, 0.0), (1.0, 10.0), (2.0, 10.0), (3.0, 0.0)), 2.5, 5.0, 1e-12),
+    (tref.PWL, ((0.0, 0.0), (1.0, 5.0), (2.0, 3.0)), 1.0, 5.0, 1e-12),      # at breakpoint
+    (tref.EXP, (0.0, 5.0, 1.0, 1.0, 3.0, 1.0), 0.5, 0.0, 1e-12),            # before td1
+    (tref.EXP, (0.0, 5.0, 0.0, 1.0, 10.0, 1.0), 1.0, 5.0 * (1.0 - math.exp(-1.0)), 1e-10),
+    (tref.EXP, (0.0, 5.0, 0.0, 1.0, 5.0, 1.0), 6.0,
+     5.0 * (1.0 - math.exp(-6.0)) - 5.0 * (1.0 - math.exp(-1.0)), 1e-10),
+]
+
+
+@pytest.mark.parametrize("case", _SOURCE_CASES, ids=lambda c: f"{c[0]}-{c[2]}")
+def test_source_functions_known_answers(case):
+    kind, params, t, expected, tol = case
+    assert abs(tref.eval_source(kind, params, t) - expected) < tol
+
+
+def test_be_companion_of_rc_step():
+    """One BE step of an RC charged through R from a 1 V step: the oracle's
+    companion system gives v = (v0 + h/(RC) * 1) / (1 + h/(RC)) (exact BE)."""
+    b = ck.CircuitBuilder()
+    b.vsource(1, 0, dc=0.0, name="V1", tran=(ck.TRAN_PULSE, (0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 2.0)))
+    b.resistors([1], [2], [1000.0])
+    b.capacitors([2], [0], [1e-9])
+    s = mna.compile_circuit(b.build())
+    x0 = np.zeros(s.size)
+    h = 1e-7
+    x, wave, _ = tref.be_transient(s, x0, 0.0, h, 3, [s.node_index(2)])
+    r = h / (1000.0 * 1e-9)
+    v = 0.0
+    for k in range(3):
+        v = (v + r * 1.0) / (1.0 + r)
+        assert abs(wave[k, 0] - v) < 1e-9 * max(1.0, abs(v))
