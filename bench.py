@@ -48,6 +48,9 @@ def parse():
                    help="Monte Carlo batch size for the batched measurement (0 skips it)")
     p.add_argument("--batch-mixed", action="store_true",
                    help="also time the batch with the FP32 Krylov bulk")
+    p.add_argument("--tran-stages", type=int, default=100_000,
+                   help="inverter-chain stages of the transient measurement (0 skips it)")
+    p.add_argument("--tran-steps", type=int, default=2000)
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                    help="one warm-up and one timed solve only (for an ncu capture)")
     return p.parse_args()
@@ -353,6 +356,8 @@ def main():
                                           "iterations, SuperLU per iteration), single thread"}
     if args.batch > 0:
         line["batch"] = batch_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+    if args.tran_stages > 0:
+        line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -463,6 +468,85 @@ def batch_section(args, S, ctx, stream, barrier, world, rank, local_rank):
                 ei = max(ei, float(np.max(np.abs(xs[i][br] - ref[br])) / max(np.max(np.abs(ref[br])), 1e-300)))
         out["rel_err_vs_oracle"] = {"voltages": ev, "currents": ei, "instances": len(sample[::2])}
     return out
+
+
+def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """CMOS inverter chain (100,000 stages, 200,000 level-1 MOSFETs, 10 fF
+    loads, PULSE input 0-1.8 V, 50 ps edges, 2 ns period): 2000 backward-Euler
+    steps of 5 ps, a Newton solve per step, all steps on the device, replayed
+    as one CUDA graph of 20 persistent launches.  Precision: FP32 Krylov bulk
+    with FP64 residual / update (and the plain FP64 path beside it)."""
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    stages, nsteps, h = args.tran_stages, args.tran_steps, 5e-12
+    sysm = mna.compile_circuit(circuits.inverter_chain(stages=stages, seed=2))
+    n = sysm.size
+    # DC operating point from logic levels (input low), then the transient
+    x0 = np.zeros(n)
+    x0[sysm.node_index(1)] = 1.8
+    out = np.array([sysm.node_index(2 + k) for k in range(1, stages + 1)])
+    x0[out] = np.where(np.arange(1, stages + 1) % 2 == 1, 1.8, 0.0)
+    plan = S.NewtonPlan(sysm, ctx)
+    x = torch.from_numpy(x0).to(f"cuda:{local_rank}")
+    dc_params = S.NewtonParams(max_iterations=100, abs_tol=1e-10, bicgstab_max_iterations=20000,
+                               bicgstab_tolerance=1e-14, inner_rtol=1e-4, continuation=True)
+    plan.newton_device(x.data_ptr(), dc_params)
+    xdc = x.clone()
+    probes = [sysm.node_index(k) for k in (2, 3, 4, 5, 102, 1002, 2 + stages)]
+    tr = S.Transient(plan, probes)
+
+    def step_params(mixed):
+        return S.NewtonParams(max_iterations=50, abs_tol=1e-9, bicgstab_max_iterations=20000,
+                              bicgstab_tolerance=1e-14, inner_rtol=1e-4, precision=1 if mixed else 0)
+
+    def timed(mixed, clk=None):
+        with torch.cuda.stream(stream):
+            x.copy_(xdc)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        wave = tr.run(x.data_ptr(), 0.0, h, nsteps, step_params(mixed), steps_per_launch=100, graph=True)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=x.device)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), dict(tr.last_info), wave
+
+    timed(True)                                     # warm-up (graph instantiation, caches)
+    with ClockSampler(local_rank) as clk:
+        ms_m, info_m, wave_m = timed(True)
+    ms_d, info_d, wave_d = timed(False)
+    res = {"workload": f"CMOS inverter chain, {stages} stages ({2 * stages} MOSFETs), {nsteps} BE steps of 5 ps",
+           "value": world * nsteps / (ms_m * 1e-3), "unit": "timesteps/s", "ms_full_run": ms_m,
+           "precision": "FP32 Krylov bulk, FP64 device evaluation / residual / update",
+           "newton_iterations": info_m["newton_iterations"], "krylov_iterations": info_m["krylov_iterations"],
+           "fp64_fallbacks": info_m["fp64_fallbacks"], "kernel_launches": info_m["launches"],
+           "cuda_graph": bool(info_m["graph"]), "clocks": clk.summary(),
+           "fp64": {"value": world * nsteps / (ms_d * 1e-3), "ms_full_run": ms_d,
+                    "newton_iterations": info_d["newton_iterations"]},
+           "mixed_vs_fp64_max_abs_diff_V": float(np.max(np.abs(wave_m - wave_d)))}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import newton_ref, transient_ref
+        xd = xdc.cpu().numpy()
+        ref_dc, _ = newton_ref.newton(sysm, x0=xd)
+        k = 3
+        t0 = time.perf_counter()
+        _, ref_wave, _ = transient_ref.be_transient(sysm, ref_dc, 0.0, h, k, probes)
+        cpu_s = time.perf_counter() - t0
+        res["rel_err_vs_oracle"] = {
+            "first_steps": k,
+            "mixed": float(np.max(np.abs(wave_m[:k] - ref_wave)) / np.max(np.abs(ref_wave))),
+            "fp64": float(np.max(np.abs(wave_d[:k] - ref_wave)) / np.max(np.abs(ref_wave))),
+            "dc_start": float(np.max(np.abs(xd[:sysm.n_nodes] - ref_dc[:sysm.n_nodes])) / 1.8)}
+        res["cpu_baseline"] = {"value": k / cpu_s, "unit": "timesteps/s", "cores": 1, "kind": "port",
+                               "sample": f"{k} BE steps of the same chain, LU Newton per step, single thread"}
+    tr.close()
+    plan.close()
+    return res
 
 
 def run_profile_case(args):
