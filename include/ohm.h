@@ -256,6 +256,33 @@ ohm_status ohm_plan_assemble(ohm_plan *plan, const double *x_host, double *value
 /* One limiting step: x_new_inout (host) is damped against x_old (host). */
 ohm_status ohm_plan_limit(ohm_plan *plan, const double *x_old_host, double *x_new_inout);
 
+/* --------------------------------------------------------------------- AC --
+ * AC sweep (src/analysis/ac.rs:25-78): for every frequency f solve
+ * (G + j 2 pi f C) x = b_ac (sparse.rs:149-178 forms the matrix; gpu.rs:210-700
+ * is the reference's complex Jacobi BiCGSTAB, one frequency at a time).  Here
+ * all points are solved by one launch, one thread block per point, in FP64
+ * complex arithmetic.  c_values lie on the pattern of g_values (NULL: no C);
+ * b and x are interleaved (re, im); x_re_im holds n_freq x n complex values.
+ * Like the reference, the devices are not linearised: pass the Jacobian
+ * values of a DC operating point as g_values for a small-signal analysis.
+ * params: tolerance / iteration limit / restarts / preconditioner (AUTO:
+ * complex block Jacobi with 2x2 blocks for branch rows; JACOBI: the
+ * reference's inverse diagonal).  Returns OHM_ERR_SOLVE naming the first
+ * point that did not converge (the reference returns its last iterate). */
+typedef struct {
+    int32_t krylov_code;         /* ohm_krylov_code */
+    int32_t iterations;
+    int32_t restarts;
+    int32_t reserved;
+    double residual_norm;        /* ||r|| of the recurrence at exit */
+    double b_norm;
+} ohm_ac_point_info;
+
+ohm_status ohm_ac_sweep(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *row_ptr, const uint32_t *col,
+                        const double *g_values, const double *c_values, const double *b_re_im, int64_t n_freq,
+                        const double *freqs_hz, const ohm_krylov_params *params, double *x_re_im,
+                        ohm_ac_point_info *points);
+
 /* -------------------------------------------------------------- transient --
  * Fixed-step backward-Euler transient with a Newton solve per step, run on
  * the device.  The reference's transient (src/analysis/transient.rs:25-210)

@@ -27,6 +27,14 @@ class KrylovParams(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class AcPointInfo(C.Structure):
+    _fields_ = [("krylov_code", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
+                ("reserved", C.c_int32), ("residual_norm", C.c_double), ("b_norm", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TransientInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("steps_done", C.c_int32), ("failed_step", C.c_int32),
                 ("krylov_code", C.c_int32), ("newton_iterations", C.c_int64), ("krylov_iterations", C.c_int64),
@@ -113,6 +121,8 @@ SIGNATURES = {
     "ohm_transient_create": (C.c_int, [_vp, _i64, _u32p, _u32p, _dp, _vp, C.c_int32, _dp, C.c_int32, _u32p,
                                        C.c_int32, C.POINTER(_vp)]),
     "ohm_transient_destroy": (C.c_int, [_vp]),
+    "ohm_ac_sweep": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64, _dp, C.POINTER(KrylovParams),
+                               _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                     C.POINTER(NewtonParamsC), C.c_int32, _dp, C.POINTER(TransientInfo)]),
     "ohm_batch_autotune": (C.c_int, [_vp, C.POINTER(NewtonParamsC), C.c_int32, C.POINTER(C.c_int32),

@@ -447,6 +447,66 @@ class NewtonBatch:
         return [a.as_dict() for a in arr]
 
 
+def ac_frequencies(sweep: str, n_points: int, f_start: float, f_stop: float) -> np.ndarray:
+    """Frequency points of an AC sweep (``generate_frequencies``,
+    src/analysis/ac.rs:80-109): DEC / OCT points per decade / octave from
+    f_start, ceil(n_points * decades) of them; LIN n_points from f_start to
+    f_stop."""
+    kind = sweep.lower()
+    if kind == "dec":
+        total = int(np.ceil(n_points * np.log10(f_stop / f_start)))
+        return np.array([f_start * 10.0 ** (i / n_points) for i in range(total)])
+    if kind == "oct":
+        total = int(np.ceil(n_points * np.log2(f_stop / f_start)))
+        return np.array([f_start * 2.0 ** (i / n_points) for i in range(total)])
+    if kind == "lin":
+        if n_points <= 1:
+            return np.array([f_start])
+        step = (f_stop - f_start) / (n_points - 1)
+        return np.array([f_start + step * i for i in range(n_points)])
+    raise InvalidArgument(f"unknown sweep type {sweep!r}")
+
+
+def ac_sweep(sysm, freqs, params: BiCgStabParams | None = None, ctx: Context | None = None, g_values=None):
+    """``analysis::ac::run`` over the given frequency points, all points in one
+    launch.  Returns (x: n_freq x size complex, per-point info)."""
+    ctx = ctx or default_context()
+    params = params or BiCgStabParams()
+    n = int(sysm.size)
+    rp, ci = _csr_u32(sysm.g)
+    g = np.ascontiguousarray(sysm.g.val if g_values is None else g_values, dtype=np.float64)
+    cv = c_on_g_pattern(sysm)
+    b = np.ascontiguousarray(np.stack([sysm.b_ac.real, sysm.b_ac.imag], axis=1).reshape(-1))
+    f = np.ascontiguousarray(freqs, dtype=np.float64)
+    x = np.zeros(2 * n * len(f))
+    pts = (_lib.AcPointInfo * max(1, len(f)))()
+    p = params.to_c()
+    st = ctx.lib.ohm_ac_sweep(ctx.handle, n, len(ci), u32ptr(rp), u32ptr(ci), dptr(g), dptr(cv), dptr(b), len(f),
+                              dptr(f), C.byref(p), dptr(x), pts)
+    infos = [pts[k].as_dict() for k in range(len(f))]
+    if st != _lib.OK:
+        _raise(st)
+    xr = x.reshape(len(f), n, 2)
+    return xr[..., 0] + 1j * xr[..., 1], infos
+
+
+def c_on_g_pattern(sysm) -> np.ndarray:
+    """C values placed on G's pattern (the compiler zero-fills G with C's
+    pattern, src/compiler.rs:576-579)."""
+    g, c = sysm.g, sysm.c
+    n = np.int64(max(int(sysm.size), 1))
+    gk = np.repeat(np.arange(g.nrows, dtype=np.int64), np.diff(g.row_ptr)) * n + g.col
+    ck = np.repeat(np.arange(c.nrows, dtype=np.int64), np.diff(c.row_ptr)) * n + c.col
+    pos = np.searchsorted(gk, ck)
+    ok = (pos < len(gk)) & (gk[np.minimum(pos, len(gk) - 1)] == ck) if len(gk) else np.zeros(len(ck), bool)
+    if not np.all(ok):
+        k = int(np.flatnonzero(~ok)[0])
+        raise CompileError(f"capacitance entry ({ck[k] // n}, {ck[k] % n}) is not on the conductance pattern")
+    out = np.zeros(g.nnz)
+    out[pos] = c.val
+    return out
+
+
 def pack_sources(sysm):
     """``ohm_source`` records and PWL points for the sources of an MnaSystem
     (``collect_source_info``, src/analysis/transient.rs:212-262): a source

@@ -383,3 +383,13 @@ def test_be_companion_of_rc_step():
     for k in range(3):
         v = (v + r * 1.0) / (1.0 + r)
         assert abs(wave[k, 0] - v) < 1e-9 * max(1.0, abs(v))
+
+
+@pytest.mark.parametrize("grid", [("dec", 10, 1e3, 1e9), ("oct", 4, 1e6, 1e10), ("lin", 25, 1e3, 1e8),
+                                  ("lin", 1, 5.0, 9.0)])
+def test_ac_frequency_grid(grid):
+    """Host-side frequency generation equals the restatement of
+    generate_frequencies (src/analysis/ac.rs:80-109)."""
+    from oracle import ac_ref
+    from ohmnivore_b200 import solver as S
+    np.testing.assert_array_equal(S.ac_frequencies(*grid), np.array(ac_ref.generate_frequencies(*grid)))
