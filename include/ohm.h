@@ -347,6 +347,57 @@ ohm_status ohm_transient_run(ohm_transient *tr, double *x_inout_device, double t
                              int32_t steps_per_launch, const ohm_newton_params *params, int32_t use_graph,
                              double *waveforms_host, ohm_transient_info *info);
 
+/* ---------------------------------------------------------------- adjoint --
+ * Sensitivities of one output o = w . x (w = do/dx, host, size n) with
+ * respect to every resistance, capacitance and diode saturation current, by
+ * the adjoint method; no counterpart in the reference.
+ *
+ * DC: J(x)^T lambda = w at the operating point x (the BiCGSTAB of this
+ * library on the transposed CSR), then do/dp = -lambda^T dF/dp, back-stamped
+ * per component: resistor (a, b, R): (v_a - v_b)(lambda_a - lambda_b) / R^2;
+ * diode: -(lambda_anode - lambda_cathode)(exp(v / nVt) - 1).
+ *
+ * Transient (backward Euler, F_n = (G + C/h) x_n - (C/h) x_{n-1} + i(x_n)
+ * - b(t_n), o = w . x_N): J_N^T lambda_N = w, J_n^T lambda_n = (C/h)^T
+ * lambda_{n+1}, then the DC start J_0^T lambda_0 = (C/h)^T lambda_1; each
+ * step back-stamps as above plus capacitor (a, b, C):
+ * -(lambda_a - lambda_b)((v_a - v_b)_n - (v_a - v_b)_{n-1}) / h.  The forward
+ * states are recomputed segment by segment from checkpoints taken every
+ * `checkpoint_every` steps.  Gradients accumulate in FP64 on the device. */
+typedef struct {
+    int64_t n_resistors;
+    const int32_t *r_a, *r_b;    /* system rows of the terminals, -1 = ground */
+    const double *r_ohms;
+    int64_t n_capacitors;
+    const int32_t *c_a, *c_b;
+    const double *c_farads;
+} ohm_components;
+
+typedef struct {
+    int32_t status;
+    int32_t steps;               /* transient steps differentiated */
+    int32_t linear_solves;       /* adjoint solves J^T lambda = rhs */
+    int32_t recompute_launches;  /* forward launches of the checkpoint recomputation */
+    int64_t krylov_iterations;   /* over the adjoint solves */
+    double output;               /* o = w . x (x_N for a transient) */
+} ohm_adjoint_info;
+
+/* DC adjoint at the operating point x_dev (device).  Gradient outputs (host,
+ * may be NULL): d_out_dr[n_resistors], d_out_dis[plan's diodes];
+ * lambda_host (may be NULL) receives lambda.  kp: FP64 Krylov settings. */
+ohm_status ohm_plan_adjoint_dc(ohm_plan *plan, const double *x_dev, const double *w_host,
+                               const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
+                               double *d_out_dis, double *lambda_host, ohm_adjoint_info *info);
+/* Transient adjoint: forward n_steps BE steps from x0_dev (the DC operating
+ * point at t0, left unchanged) with Newton params np, then the reverse
+ * sweep.  Outputs (host, may be NULL): d_out_dr, d_out_dc[n_capacitors],
+ * d_out_dis.  Includes the dependence of x0 on the parameters (the DC
+ * adjoint at the start). */
+ohm_status ohm_transient_adjoint(ohm_transient *tr, const double *x0_dev, double t0, double h, int32_t n_steps,
+                                 int32_t checkpoint_every, const ohm_newton_params *np, const double *w_host,
+                                 const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
+                                 double *d_out_dc, double *d_out_dis, ohm_adjoint_info *info);
+
 /* ---------------------------------------------------------------- batches --
  * Many independent nonlinear circuits solved by one launch (Monte Carlo
  * corners, parameter sweeps).  No counterpart in the reference, which runs

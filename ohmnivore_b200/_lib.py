@@ -27,6 +27,19 @@ class KrylovParams(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class Components(C.Structure):
+    _fields_ = [("n_resistors", C.c_int64), ("r_a", C.c_void_p), ("r_b", C.c_void_p), ("r_ohms", C.c_void_p),
+                ("n_capacitors", C.c_int64), ("c_a", C.c_void_p), ("c_b", C.c_void_p), ("c_farads", C.c_void_p)]
+
+
+class AdjointInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("steps", C.c_int32), ("linear_solves", C.c_int32),
+                ("recompute_launches", C.c_int32), ("krylov_iterations", C.c_int64), ("output", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class AcPointInfo(C.Structure):
     _fields_ = [("krylov_code", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
                 ("reserved", C.c_int32), ("residual_norm", C.c_double), ("b_norm", C.c_double)]
@@ -121,6 +134,11 @@ SIGNATURES = {
     "ohm_transient_create": (C.c_int, [_vp, _i64, _u32p, _u32p, _dp, _vp, C.c_int32, _dp, C.c_int32, _u32p,
                                        C.c_int32, C.POINTER(_vp)]),
     "ohm_transient_destroy": (C.c_int, [_vp]),
+    "ohm_plan_adjoint_dc": (C.c_int, [_vp, _vp, _dp, C.POINTER(Components), C.POINTER(KrylovParams), _dp, _dp, _dp,
+                                      C.POINTER(AdjointInfo)]),
+    "ohm_transient_adjoint": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                        C.POINTER(NewtonParamsC), _dp, C.POINTER(Components),
+                                        C.POINTER(KrylovParams), _dp, _dp, _dp, C.POINTER(AdjointInfo)]),
     "ohm_ac_sweep": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64, _dp, C.POINTER(KrylovParams),
                                _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,

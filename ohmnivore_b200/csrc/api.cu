@@ -993,6 +993,97 @@ extern "C" ohm_status ohm_plan_assemble(ohm_plan *p, const double *x_host, doubl
     return ohm_plan_download_system(p, values_out, rhs_out);
 }
 
+// ------------------------------------------------ internal: adjoint support --
+ohm_status ohm_plan_jacobian_device(ohm_plan *p, const double *x_dev, const double *base_vals_dev, double *J_out) {
+    if (!p || !x_dev || !J_out) return fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_ctx *c = p->ctx;
+    cudaStream_t s = c->stream;
+    ohm_newton_params np;
+    ohm_newton_params_default(&np);
+    KernelArgs a;
+    ohm_status st = plan_args(p, &np, const_cast<double *>(x_dev), a);
+    if (st != OHM_OK) return st;
+    a.base_vals = base_vals_dev ? base_vals_dev : p->base_vals;
+    a.vals64 = J_out;
+    a.vals32 = nullptr;
+    if (p->nnz) CUDA_TRY(cudaMemcpyAsync(J_out, a.base_vals, p->nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const int64_t ndev = p->nd + p->nq + p->nm;
+    if (ndev) eval_devices_kernel<<<steps_grid(ndev), 256, 0, s>>>(a);
+    if (p->n_mslots + p->n_rrows) assemble_kernel<<<steps_grid(p->n_mslots + p->n_rrows), 256, 0, s>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return OHM_OK;
+}
+
+struct ohm_linsys {
+    ohm_ctx *ctx = nullptr;
+    int64_t n = 0, nnz = 0;
+    uint32_t *rp = nullptr, *col = nullptr;
+    Workspace ws;
+};
+
+ohm_status ohm_linsys_create(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *h_rp, const uint32_t *h_col,
+                             const double *h_val, ohm_linsys **out) {
+    if (!c || !out) return fail(OHM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    ohm_status st = check_csr(n, nnz, h_rp, h_col);
+    if (st != OHM_OK) return st;
+    ohm_linsys *L = new ohm_linsys();
+    L->ctx = c; L->n = n; L->nnz = nnz;
+    PcHost pc;
+    build_precond(n, h_rp, h_col, h_val, {}, true, pc);
+    cudaError_t e = dalloc(&L->rp, n + 1);
+    if (e == cudaSuccess) e = dalloc(&L->col, nnz);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L->rp, h_rp, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(L->col, h_col, nnz * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = L->ws.alloc(n, c->num_sms);
+    if (e == cudaSuccess) e = L->ws.upload_pc(pc, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        ohm_linsys_destroy(L);
+        return fail(OHM_ERR_CUDA, "linear system set-up: %s", cudaGetErrorString(e));
+    }
+    *out = L;
+    return OHM_OK;
+}
+
+ohm_status ohm_linsys_solve(ohm_linsys *L, double *d_vals, double *d_b, double *d_x, const ohm_krylov_params *p,
+                            ohm_solve_info *info) {
+    ohm_status st = ohm_check_krylov(p);
+    if (st != OHM_OK) return st;
+    if (p->precision != OHM_PREC_FP64 || p->precond == OHM_PRECOND_ISAI1)
+        return fail(OHM_ERR_INVALID_ARG, "adjoint solves run in FP64 with block Jacobi, Jacobi or none");
+    ohm_ctx *c = L->ctx;
+    CUDA_TRY(cudaMemsetAsync(d_x, 0, L->n * sizeof(double), c->stream));
+    KernelArgs a{};
+    a.n = (int)L->n; a.nnz = (int)L->nnz;
+    a.row_ptr = L->rp; a.col = L->col; a.vals64 = d_vals; a.vals32 = nullptr;
+    a.b = d_b; a.x = d_x;
+    a.precond = precond_kind(p->precond);
+    L->ws.bind(a);
+    a.newton = 0;
+    a.mixed = 0;
+    a.max_outer = 1;
+    a.max_krylov = p->max_iterations;
+    a.krylov_tol = p->tolerance;
+    a.inner_rtol = p->inner_rtol;
+    a.max_restarts = std::max(0, p->max_restarts);
+    a.fp32_max_iterations = p->max_iterations;
+    a.eta_max = 0.5;
+    int launches = 0;
+    st = launch_solver(c, a, L->nnz, &launches);
+    if (st == OHM_OK) st = finish_solver(c, info, launches);
+    return st;
+}
+
+void ohm_linsys_destroy(ohm_linsys *L) {
+    if (!L) return;
+    cudaStreamSynchronize(L->ctx->stream);
+    cudaFree(L->rp);
+    cudaFree(L->col);
+    L->ws.release();
+    delete L;
+}
+
 extern "C" ohm_status ohm_plan_download_system(ohm_plan *p, double *values, double *rhs) {
     if (!p) return fail(OHM_ERR_INVALID_ARG, "plan is null");
     cudaStream_t s = p->ctx->stream;

@@ -55,6 +55,18 @@ ohm_status ohm_check_krylov(const ohm_krylov_params *p);
 ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, ohm::KernelArgs &a,
                                 int64_t *nnz);
 ohm_ctx *ohm_plan_context(ohm_plan *p);
+// J(x) values of a plan's system at a device x, on base values base_vals_dev
+// (the plan's conductance base when null), written to J_out (nnz doubles).
+ohm_status ohm_plan_jacobian_device(ohm_plan *p, const double *x_dev, const double *base_vals_dev, double *J_out);
+// A device linear system of fixed pattern (uploaded once, with its
+// preconditioner structure and Krylov workspace) solved for new values and
+// right-hand sides; FP64.  x starts from zero.
+struct ohm_linsys;
+ohm_status ohm_linsys_create(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *h_rp, const uint32_t *h_col,
+                             const double *h_val, ohm_linsys **out);
+ohm_status ohm_linsys_solve(ohm_linsys *L, double *d_vals, double *d_b, double *d_x, const ohm_krylov_params *p,
+                            ohm_solve_info *info);
+void ohm_linsys_destroy(ohm_linsys *L);
 cudaError_t ohm_f64_to_f32(const double *in, float *out, int64_t n, cudaStream_t s);
 
 // Child-object bookkeeping (see ohm_ctx::live_objects).

@@ -46,6 +46,8 @@ struct TranArgs {
     double *wave;                      // n_steps x n_probes
     double *beff;                      // base rhs of the current step
     TranDev *st;
+    double *states;                    // optional: x after step s at (s - state_base) * n
+    int state_base;
 };
 
 // Source waveforms, the formulas of transient_source.rs:39-118.
@@ -149,6 +151,10 @@ __global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a
         if (o.status != kOk) return;
         for (int k = g.gtid; k < T.n_probes; k += g.gstride)
             T.wave[(size_t)s * T.n_probes + k] = a.x[T.probe[k]];
+        if (T.states) {
+            double *st = T.states + (size_t)(s - T.state_base) * a.n;
+            for (int i = g.r0 + threadIdx.x; i < g.r1; i += blockDim.x) st[i] = a.x[i];
+        }
     }
 }
 
@@ -325,32 +331,16 @@ extern "C" ohm_status ohm_transient_destroy(ohm_transient *t) {
     return OHM_OK;
 }
 
-extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double t0, double h, int32_t n_steps,
-                                        int32_t steps_per_launch, const ohm_newton_params *np, int32_t use_graph,
-                                        double *waveforms_host, ohm_transient_info *info) {
-    if (!t || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
-    if (!(h > 0.0) || n_steps < 0 || steps_per_launch <= 0)
-        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 0, steps_per_launch > 0");
-    if (np->continuation) return ohm_fail(OHM_ERR_INVALID_ARG, "continuation is for DC solves, not transient steps");
-    if (np->krylov.precond == OHM_PRECOND_ISAI1)
-        return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi");
+// Kernel arguments of a run on x_dev with step h: the companion base
+// A = G + C/h is formed (and copied to the assembled arrays), the run
+// record zeroed.  Returns the kernel and grid to launch.
+static ohm_status tran_prepare(ohm_transient *t, double *x_dev, double h, const ohm_newton_params *np,
+                               KernelArgs &a, TranArgs &T, TranFn &fn, int &grid, const double *&G) {
     ohm_ctx *c = t->ctx;
-    KernelArgs a;
     int64_t nnz = 0;
     ohm_status st = ohm_plan_kernel_args(t->plan, np, x_dev, a, &nnz);
     if (st != OHM_OK) return st;
-    if (np->initial_guess)
-        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    const int64_t need = (int64_t)n_steps * t->n_probes;
-    if (need > t->wave_cap) {
-        cudaFree(t->wave);
-        t->wave = nullptr;
-        t->wave_cap = 0;
-        CUDA_TRY(dalloc(&t->wave, (size_t)need));
-        t->wave_cap = need;
-    }
-    // companion base A = G + C/h, assembled arrays start from it
-    const double *G = a.base_vals;
+    G = a.base_vals;
     for (int phase = 0; phase < 3; ++phase) {
         companion_kernel<<<steps_grid(phase == 1 ? t->c_nnz : nnz), 256, 0, c->stream>>>(
             G, t->aval, a.vals64, a.vals32, nnz, t->c_slot, t->c_val, t->c_nnz, 1.0 / h, phase);
@@ -361,45 +351,96 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
     a.base_b = t->beff;
     a.trace = nullptr;
     a.continuation = 0;
-
-    TranArgs T{};
-    T.t0 = t0; T.h = h;
+    T = TranArgs{};
+    T.h = h;
     T.c_rp = t->c_rp; T.c_col = t->c_col; T.c_val = t->c_val;
     T.src_of_row = t->src_of_row; T.srow_ptr = t->srow_ptr; T.srow_src = t->srow_src; T.srow_sign = t->srow_sign;
     T.src = t->src; T.pwl = t->pwl; T.probe = t->probe; T.n_probes = t->n_probes; T.wave = t->wave;
     T.beff = t->beff; T.st = t->st;
-
-    // grid: as for the persistent Newton solver
-    TranFn fn = pick_tran(tran_lpr(t->n, nnz));
+    fn = pick_tran(tran_lpr(t->n, nnz));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0));
     if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "transient kernel does not fit on an SM");
     per_sm = std::min(per_sm, 2);
     int64_t want = (t->n + kSolverBlock - 1) / kSolverBlock;
     want = std::max<int64_t>(want, ((int64_t)a.nd + a.nq + a.nm + kSolverBlock - 1) / kSolverBlock);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
+    grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
     a.gs.count = (unsigned long long *)c->sync_words;
     a.gs.error = (int *)(c->sync_words + 2);
     a.info = c->info_dev;
+    return OHM_OK;
+}
 
+// One cooperative launch of steps [s0, s1).
+static cudaError_t tran_launch(ohm_ctx *c, TranFn fn, int grid, const KernelArgs &a, TranArgs T, int s0, int s1) {
+    T.s0 = s0;
+    T.s1 = s1;
+    cudaError_t e = cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kSolverBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, a, T);
+}
+
+// Status of a run from the device record and the barrier error word.
+static ohm_status tran_status(ohm_transient *t, double t0, double h, TranDev &d) {
+    ohm_ctx *c = t->ctx;
+    unsigned int words[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(&d, t->st, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (words[2] != 0) return ohm_fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
+    if (d.status != 0)
+        return ohm_fail(d.status == kErrSolve ? OHM_ERR_SOLVE
+                        : (d.status == kErrNewtonNumerical ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
+                        "transient step %d at t = %.6e failed (status %d, krylov code %d)", d.failed_step,
+                        t0 + (d.failed_step + 1) * h, d.status, d.kcode);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double t0, double h, int32_t n_steps,
+                                        int32_t steps_per_launch, const ohm_newton_params *np, int32_t use_graph,
+                                        double *waveforms_host, ohm_transient_info *info) {
+    if (!t || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (!(h > 0.0) || n_steps < 0 || steps_per_launch <= 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 0, steps_per_launch > 0");
+    if (np->continuation) return ohm_fail(OHM_ERR_INVALID_ARG, "continuation is for DC solves, not transient steps");
+    if (np->krylov.precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi");
+    ohm_ctx *c = t->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (np->initial_guess)
+        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int64_t need = (int64_t)n_steps * t->n_probes;
+    if (need > t->wave_cap) {
+        cudaFree(t->wave);
+        t->wave = nullptr;
+        t->wave_cap = 0;
+        CUDA_TRY(dalloc(&t->wave, (size_t)need));
+        t->wave_cap = need;
+    }
+    KernelArgs a;
+    TranArgs T;
+    TranFn fn = nullptr;
+    int grid = 0;
+    const double *G = nullptr;
+    ohm_status st = tran_prepare(t, x_dev, h, np, a, T, fn, grid, G);
+    if (st != OHM_OK) return st;
+    T.t0 = t0;
+    const int64_t nnz = t->nnz;
     const int n_launch = (n_steps + steps_per_launch - 1) / steps_per_launch;
     auto enqueue = [&]() -> cudaError_t {
         for (int l = 0; l < n_launch; ++l) {
-            T.s0 = l * steps_per_launch;
-            T.s1 = std::min(n_steps, T.s0 + steps_per_launch);
-            cudaError_t e = cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream);
-            if (e != cudaSuccess) return e;
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(kSolverBlock);
-            cfg.dynamicSmemBytes = 0;
-            cfg.stream = c->stream;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeCooperative;
-            attr[0].val.cooperative = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            e = cudaLaunchKernelEx(&cfg, fn, a, T);
+            const int s0 = l * steps_per_launch;
+            cudaError_t e = tran_launch(c, fn, grid, a, T, s0, std::min(n_steps, s0 + steps_per_launch));
             if (e != cudaSuccess) return e;
         }
         if (waveforms_host && need)
@@ -431,19 +472,7 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
     restore_kernel<<<steps_grid(nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, nnz);
     CUDA_TRY(cudaGetLastError());
     TranDev d{};
-    unsigned int words[4] = {0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpyAsync(&d, t->st, sizeof d, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
-    ohm_status rs = OHM_OK;
-    if (words[2] != 0) {
-        rs = ohm_fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
-    } else if (d.status != 0) {
-        rs = ohm_fail(d.status == kErrSolve ? OHM_ERR_SOLVE
-                      : (d.status == kErrNewtonNumerical ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
-                      "transient step %d at t = %.6e failed (status %d, krylov code %d)", d.failed_step,
-                      t0 + (d.failed_step + 1) * h, d.status, d.kcode);
-    }
+    const ohm_status rs = tran_status(t, t0, h, d);
     if (info) {
         std::memset(info, 0, sizeof *info);
         info->status = rs;
@@ -458,4 +487,335 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
         info->max_residual = d.max_residual;
     }
     return rs;
+}
+
+// ================================================================= adjoint ==
+namespace {
+
+struct BackArgs {
+    const double *x, *xprev, *lam;     // xprev null: DC (no capacitor term)
+    double inv_h;
+    int64_t nr, nc, nd;
+    const int32_t *ra, *rb, *ca, *cb;
+    const double *rv, *cv;
+    const DiodeDesc *dio;
+    double *gr, *gc, *gd;
+};
+
+__device__ __forceinline__ double at(const double *v, int32_t i) { return i >= 0 ? v[i] : 0.0; }
+
+// do/dp += -lambda^T dF/dp for every component, one thread per component
+// (accumulation over steps in launch order: deterministic).
+__global__ void backstamp_kernel(BackArgs B) {
+    const int64_t total = B.nr + (B.xprev ? B.nc : 0) + B.nd;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        if (k < B.nr) {
+            const int32_t a = B.ra[k], b = B.rb[k];
+            const double r = B.rv[k];
+            B.gr[k] += (at(B.x, a) - at(B.x, b)) * (at(B.lam, a) - at(B.lam, b)) / (r * r);
+            continue;
+        }
+        int64_t q = k - B.nr;
+        if (B.xprev) {
+            if (q < B.nc) {
+                const int32_t a = B.ca[q], b = B.cb[q];
+                const double dv = (at(B.x, a) - at(B.x, b)) - (at(B.xprev, a) - at(B.xprev, b));
+                B.gc[q] -= dv * B.inv_h * (at(B.lam, a) - at(B.lam, b));
+                continue;
+            }
+            q -= B.nc;
+        }
+        const DiodeDesc &d = B.dio[q];
+        const double v = node_v(B.x, d.anode) - node_v(B.x, d.cathode);
+        const double e = clamp_exp(v / (double)d.n_vt);
+        B.gd[q] -= (node_v(B.lam, d.anode) - node_v(B.lam, d.cathode)) * (e - 1.0);
+    }
+}
+
+__global__ void gather_kernel(double *dst, const double *src, const uint32_t *perm, int64_t m) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[perm[k]];
+}
+
+// rhs = (C/h)^T lambda, C^T in CSR
+__global__ void ct_rhs_kernel(double *rhs, const uint32_t *rp, const uint32_t *col, const double *val,
+                              const double *lam, double inv_h, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) acc += val[k] * lam[col[k]];
+        rhs[i] = acc * inv_h;
+    }
+}
+
+// Transposed CSR of a pattern: t_rp, t_col and perm (t slot -> source slot).
+void transpose_pattern(int64_t n, const std::vector<uint32_t> &rp, const std::vector<uint32_t> &col,
+                       std::vector<uint32_t> &t_rp, std::vector<uint32_t> &t_col, std::vector<uint32_t> &perm) {
+    const int64_t nnz = (int64_t)col.size();
+    t_rp.assign(n + 1, 0);
+    for (int64_t k = 0; k < nnz; ++k) ++t_rp[col[k] + 1];
+    for (int64_t i = 0; i < n; ++i) t_rp[i + 1] += t_rp[i];
+    t_col.assign(nnz, 0);
+    perm.assign(nnz, 0);
+    std::vector<uint32_t> fill(t_rp.begin(), t_rp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const uint32_t d = fill[col[k]]++;
+            t_col[d] = (uint32_t)i;
+            perm[d] = k;
+        }
+}
+
+// Device state of one adjoint computation (freed on destruction).
+struct AdjointCtx {
+    ohm_ctx *c = nullptr;
+    std::vector<void *> allocs;
+    ohm_linsys *L = nullptr;
+    int64_t n = 0, nnz = 0;
+    uint32_t *perm = nullptr;
+    double *J = nullptr, *JT = nullptr, *lam = nullptr, *rhs = nullptr;
+    BackArgs B{};
+    ~AdjointCtx() {
+        if (c) cudaStreamSynchronize(c->stream);
+        ohm_linsys_destroy(L);
+        for (void *p : allocs) cudaFree(p);
+    }
+    template <typename T>
+    cudaError_t put(T **dst, const T *h, size_t count) {
+        cudaError_t e = dalloc(dst, count);
+        if (e == cudaSuccess) allocs.push_back((void *)*dst);
+        if (e == cudaSuccess && count) {
+            if (h) e = cudaMemcpyAsync(*dst, h, count * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+            else e = cudaMemsetAsync(*dst, 0, count * sizeof(T), c->stream);
+        }
+        return e;
+    }
+
+    // pattern transpose, J^T linear system, component arrays, accumulators
+    ohm_status setup(ohm_plan *plan, const ohm_components *comps, const KernelArgs &a, int64_t nnz_) {
+        c = ohm_plan_context(plan);
+        n = a.n;
+        nnz = nnz_;
+        if (comps && ((comps->n_resistors && (!comps->r_a || !comps->r_b || !comps->r_ohms)) ||
+                      (comps->n_capacitors && (!comps->c_a || !comps->c_b || !comps->c_farads))))
+            return ohm_fail(OHM_ERR_INVALID_ARG, "null component array");
+        const int64_t nr = comps ? comps->n_resistors : 0, nc = comps ? comps->n_capacitors : 0;
+        for (int64_t k = 0; k < nr; ++k)
+            if (comps->r_a[k] < -1 || comps->r_a[k] >= n || comps->r_b[k] < -1 || comps->r_b[k] >= n)
+                return ohm_fail(OHM_ERR_INVALID_ARG, "resistor %lld: row out of range", (long long)k);
+        for (int64_t k = 0; k < nc; ++k)
+            if (comps->c_a[k] < -1 || comps->c_a[k] >= n || comps->c_b[k] < -1 || comps->c_b[k] >= n)
+                return ohm_fail(OHM_ERR_INVALID_ARG, "capacitor %lld: row out of range", (long long)k);
+        std::vector<uint32_t> rp(n + 1), col(nnz), t_rp, t_col, pm;
+        std::vector<double> g(nnz), gt(nnz);
+        CUDA_TRY(cudaMemcpy(rp.data(), a.row_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (nnz) CUDA_TRY(cudaMemcpy(col.data(), a.col, nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (nnz) CUDA_TRY(cudaMemcpy(g.data(), a.base_vals, nnz * sizeof(double), cudaMemcpyDeviceToHost));
+        transpose_pattern(n, rp, col, t_rp, t_col, pm);
+        for (int64_t k = 0; k < nnz; ++k) gt[k] = g[pm[k]];
+        ohm_status st = ohm_linsys_create(c, n, nnz, t_rp.data(), t_col.data(), gt.data(), &L);
+        if (st != OHM_OK) return st;
+        cudaError_t e = put(&perm, pm.data(), nnz);
+        if (e == cudaSuccess) e = put(&J, (const double *)nullptr, nnz);
+        if (e == cudaSuccess) e = put(&JT, (const double *)nullptr, nnz);
+        if (e == cudaSuccess) e = put(&lam, (const double *)nullptr, n);
+        if (e == cudaSuccess) e = put(&rhs, (const double *)nullptr, n);
+        int32_t *i32 = nullptr;
+        double *f64 = nullptr;
+        B = BackArgs{};
+        B.nr = nr; B.nc = nc; B.nd = a.nd; B.dio = a.diodes;
+        if (e == cudaSuccess && nr) { e = put(&i32, comps->r_a, nr); B.ra = i32; }
+        if (e == cudaSuccess && nr) { e = put(&i32, comps->r_b, nr); B.rb = i32; }
+        if (e == cudaSuccess && nr) { e = put(&f64, comps->r_ohms, nr); B.rv = f64; }
+        if (e == cudaSuccess && nc) { e = put(&i32, comps->c_a, nc); B.ca = i32; }
+        if (e == cudaSuccess && nc) { e = put(&i32, comps->c_b, nc); B.cb = i32; }
+        if (e == cudaSuccess && nc) { e = put(&f64, comps->c_farads, nc); B.cv = f64; }
+        if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(nr, 1)); B.gr = f64; }
+        if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(nc, 1)); B.gc = f64; }
+        if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(a.nd, 1)); B.gd = f64; }
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "adjoint set-up: %s", cudaGetErrorString(e));
+        B.lam = lam;
+        return OHM_OK;
+    }
+
+    // J(x)^T lam = rhs on base values `base`, then the back-stamp at (x, xprev).
+    ohm_status step(ohm_plan *plan, const double *x, const double *xprev, const double *base, double inv_h,
+                    const ohm_krylov_params *kp, int64_t &kiters) {
+        ohm_status st = ohm_plan_jacobian_device(plan, x, base, J);
+        if (st != OHM_OK) return st;
+        gather_kernel<<<steps_grid(nnz), 256, 0, c->stream>>>(JT, J, perm, nnz);
+        CUDA_TRY(cudaGetLastError());
+        ohm_solve_info si{};
+        st = ohm_linsys_solve(L, JT, rhs, lam, kp, &si);
+        kiters += si.krylov_iterations;
+        if (st != OHM_OK) return st;
+        BackArgs b = B;
+        b.x = x;
+        b.xprev = xprev;
+        b.inv_h = inv_h;
+        const int64_t total = b.nr + (xprev ? b.nc : 0) + b.nd;
+        if (total) backstamp_kernel<<<steps_grid(total), 256, 0, c->stream>>>(b);
+        CUDA_TRY(cudaGetLastError());
+        return OHM_OK;
+    }
+
+    ohm_status download(double *gr, double *gc, double *gd, double *lam_host) {
+        if (gr && B.nr) CUDA_TRY(cudaMemcpyAsync(gr, B.gr, B.nr * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (gc && B.nc) CUDA_TRY(cudaMemcpyAsync(gc, B.gc, B.nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (gd && B.nd) CUDA_TRY(cudaMemcpyAsync(gd, B.gd, B.nd * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (lam_host) CUDA_TRY(cudaMemcpyAsync(lam_host, lam, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return OHM_OK;
+    }
+};
+
+double host_dot(ohm_ctx *c, const double *w, const double *x_dev, int64_t n) {
+    std::vector<double> x(n);
+    if (cudaMemcpyAsync(x.data(), x_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return NAN;
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += w[i] * x[i];
+    return s;
+}
+
+}  // namespace
+
+extern "C" ohm_status ohm_plan_adjoint_dc(ohm_plan *plan, const double *x_dev, const double *w_host,
+                                          const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
+                                          double *d_out_dis, double *lambda_host, ohm_adjoint_info *info) {
+    if (!plan || !x_dev || !w_host || !kp) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    ohm_newton_params np;
+    ohm_newton_params_default(&np);
+    KernelArgs a;
+    int64_t nnz = 0;
+    ohm_status st = ohm_plan_kernel_args(plan, &np, const_cast<double *>(x_dev), a, &nnz);
+    if (st != OHM_OK) return st;
+    AdjointCtx A;
+    st = A.setup(plan, comps, a, nnz);
+    if (st != OHM_OK) return st;
+    ohm_ctx *c = A.c;
+    CUDA_TRY(cudaMemcpyAsync(A.rhs, w_host, a.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int64_t kiters = 0;
+    st = A.step(plan, x_dev, nullptr, nullptr, 0.0, kp, kiters);
+    if (st == OHM_OK) st = A.download(d_out_dr, nullptr, d_out_dis, lambda_host);
+    if (info) {
+        std::memset(info, 0, sizeof *info);
+        info->status = st;
+        info->linear_solves = 1;
+        info->krylov_iterations = kiters;
+        info->output = host_dot(c, w_host, x_dev, a.n);
+    }
+    return st;
+}
+
+extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_dev, double t0, double h,
+                                            int32_t n_steps, int32_t checkpoint_every, const ohm_newton_params *np,
+                                            const double *w_host, const ohm_components *comps,
+                                            const ohm_krylov_params *kp, double *d_out_dr, double *d_out_dc,
+                                            double *d_out_dis, ohm_adjoint_info *info) {
+    if (!t || !x0_dev || !np || !w_host || !kp) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (!(h > 0.0) || n_steps < 1 || checkpoint_every < 1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 1, checkpoint_every >= 1");
+    if (np->continuation || np->krylov.precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi, no continuation");
+    ohm_ctx *c = t->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int64_t n = t->n;
+    const int K = checkpoint_every;
+    const int nseg = (n_steps + K - 1) / K;
+    AdjointCtx A;
+    double *x = nullptr, *ck = nullptr, *S = nullptr;
+    {
+        KernelArgs a0;
+        int64_t nnz = 0;
+        ohm_newton_params dp;
+        ohm_newton_params_default(&dp);
+        ohm_status st = ohm_plan_kernel_args(t->plan, &dp, const_cast<double *>(x0_dev), a0, &nnz);
+        if (st != OHM_OK) return st;
+        st = A.setup(t->plan, comps, a0, nnz);
+        if (st != OHM_OK) return st;
+    }
+    cudaError_t e = A.put(&x, (const double *)nullptr, n);
+    if (e == cudaSuccess) e = A.put(&ck, (const double *)nullptr, (size_t)nseg * n);
+    if (e == cudaSuccess) e = A.put(&S, (const double *)nullptr, (size_t)K * n);
+    if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "adjoint buffers: %s", cudaGetErrorString(e));
+    // C^T for the adjoint recursion
+    std::vector<uint32_t> crp(n + 1), ccol(t->c_nnz), ctrp, ctcol, cpm;
+    std::vector<double> cval(t->c_nnz), ctval(t->c_nnz);
+    CUDA_TRY(cudaMemcpy(crp.data(), t->c_rp, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (t->c_nnz) {
+        CUDA_TRY(cudaMemcpy(ccol.data(), t->c_col, t->c_nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(cval.data(), t->c_val, t->c_nnz * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    transpose_pattern(n, crp, ccol, ctrp, ctcol, cpm);
+    for (int64_t k = 0; k < t->c_nnz; ++k) ctval[k] = cval[cpm[k]];
+    uint32_t *d_ctrp = nullptr, *d_ctcol = nullptr;
+    double *d_ctval = nullptr;
+    e = A.put(&d_ctrp, ctrp.data(), n + 1);
+    if (e == cudaSuccess) e = A.put(&d_ctcol, ctcol.data(), t->c_nnz);
+    if (e == cudaSuccess) e = A.put(&d_ctval, ctval.data(), t->c_nnz);
+    if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "adjoint buffers: %s", cudaGetErrorString(e));
+
+    // ---- forward, checkpoint at the start of every segment ----
+    KernelArgs a;
+    TranArgs T;
+    TranFn fn = nullptr;
+    int grid = 0;
+    const double *G = nullptr;
+    CUDA_TRY(cudaMemcpyAsync(x, x0_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    ohm_status st = tran_prepare(t, x, h, np, a, T, fn, grid, G);
+    if (st != OHM_OK) return st;
+    T.t0 = t0;
+    T.n_probes = 0;
+    int launches = 0;
+    for (int sg = 0; sg < nseg; ++sg) {
+        CUDA_TRY(cudaMemcpyAsync(ck + (size_t)sg * n, x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(tran_launch(c, fn, grid, a, T, sg * K, std::min(n_steps, (sg + 1) * K)));
+    }
+    TranDev d{};
+    st = tran_status(t, t0, h, d);
+    double output = NAN;
+    if (st == OHM_OK) output = host_dot(c, w_host, x, n);
+    // ---- reverse sweep ----
+    int64_t kiters = 0;
+    int solves = 0;
+    if (st == OHM_OK) CUDA_TRY(cudaMemcpyAsync(A.rhs, w_host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double inv_h = 1.0 / h;
+    for (int sg = nseg - 1; st == OHM_OK && sg >= 0; --sg) {
+        const int s0 = sg * K, s1 = std::min(n_steps, (sg + 1) * K);
+        // recompute x_{s0+1} .. x_{s1} from the checkpoint x_{s0}
+        CUDA_TRY(cudaMemcpyAsync(x, ck + (size_t)sg * n, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        T.states = S;
+        T.state_base = s0;
+        CUDA_TRY(tran_launch(c, fn, grid, a, T, s0, s1));
+        ++launches;
+        st = tran_status(t, t0, h, d);
+        for (int s = s1 - 1; st == OHM_OK && s >= s0; --s) {
+            // step s maps x_s (state index s, or the checkpoint) to x_{s+1}
+            const double *xn = S + (size_t)(s - s0) * n;
+            const double *xp = s == s0 ? ck + (size_t)sg * n : S + (size_t)(s - s0 - 1) * n;
+            st = A.step(t->plan, xn, xp, t->aval, inv_h, kp, kiters);
+            ++solves;
+            if (st != OHM_OK) break;
+            ct_rhs_kernel<<<steps_grid(n), 256, 0, c->stream>>>(A.rhs, d_ctrp, d_ctcol, d_ctval, A.lam, inv_h, n);
+            CUDA_TRY(cudaGetLastError());
+        }
+    }
+    // ---- the DC start: J_0^T lambda_0 = (C/h)^T lambda_1 ----
+    if (st == OHM_OK) {
+        st = A.step(t->plan, ck, nullptr, nullptr, 0.0, kp, kiters);
+        ++solves;
+    }
+    restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
+    if (st == OHM_OK) st = A.download(d_out_dr, d_out_dc, d_out_dis, nullptr);
+    if (info) {
+        std::memset(info, 0, sizeof *info);
+        info->status = st;
+        info->steps = n_steps;
+        info->linear_solves = solves;
+        info->recompute_launches = launches;
+        info->krylov_iterations = kiters;
+        info->output = output;
+    }
+    return st;
 }

@@ -507,6 +507,55 @@ def c_on_g_pattern(sysm) -> np.ndarray:
     return out
 
 
+class ComponentTable:
+    """Resistors and capacitors of a circuit as system rows (-1 = ground) and
+    values, in circuit order (the parameters the adjoint differentiates)."""
+
+    def __init__(self, ckt, sysm):
+        from . import circuits as ck
+        labels = np.asarray(sysm.node_labels, dtype=np.int64)
+        order = np.argsort(labels, kind="stable")
+        sl = labels[order]
+
+        def rows(lab):
+            lab = np.asarray(lab, dtype=np.int64)
+            if not len(sl):
+                return np.full(lab.shape, -1, np.int32)
+            pos = np.minimum(np.searchsorted(sl, lab), len(sl) - 1)
+            ok = (lab != 0) & (sl[pos] == lab)
+            return np.where(ok, order[pos], -1).astype(np.int32)
+
+        r = np.flatnonzero(ckt.kind == ck.R)
+        c = np.flatnonzero(ckt.kind == ck.C)
+        self.r_index, self.c_index = r, c
+        self.r_a, self.r_b = rows(ckt.nodes[r, 0]), rows(ckt.nodes[r, 1])
+        self.r_ohms = np.ascontiguousarray(ckt.value[r], dtype=np.float64)
+        self.c_a, self.c_b = rows(ckt.nodes[c, 0]), rows(ckt.nodes[c, 1])
+        self.c_farads = np.ascontiguousarray(ckt.value[c], dtype=np.float64)
+
+    def to_c(self):
+        return _lib.Components(len(self.r_ohms), vptr(self.r_a), vptr(self.r_b), vptr(self.r_ohms),
+                               len(self.c_farads), vptr(self.c_a), vptr(self.c_b), vptr(self.c_farads))
+
+
+def adjoint_dc(plan: "NewtonPlan", x_dev_ptr: int, w, comps: ComponentTable, params: BiCgStabParams | None = None):
+    """do/dp of o = w . x at the DC operating point x (device pointer) for
+    every resistor and diode Is.  Returns (dict of gradients, lambda, info)."""
+    kp = (params or BiCgStabParams(max_iterations=20000, tolerance=1e-14)).to_c()
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    gr = np.zeros(len(comps.r_ohms))
+    gd = np.zeros(len(plan.sysm.diode_descriptors))
+    lam = np.zeros(plan.n)
+    info = _lib.AdjointInfo()
+    cc = comps.to_c()
+    st = plan.ctx.lib.ohm_plan_adjoint_dc(plan._h, C.c_void_p(int(x_dev_ptr)), dptr(w), C.byref(cc), C.byref(kp),
+                                          dptr(gr) if len(gr) else None, dptr(gd) if len(gd) else None, dptr(lam),
+                                          C.byref(info))
+    if st != _lib.OK:
+        _raise(st)
+    return {"R": gr, "Is": gd}, lam, info.as_dict()
+
+
 def pack_sources(sysm):
     """``ohm_source`` records and PWL points for the sources of an MnaSystem
     (``collect_source_info``, src/analysis/transient.rs:212-262): a source
@@ -573,6 +622,30 @@ class Transient:
             self.close()
         except Exception:
             pass
+
+    def adjoint(self, x0_dev_ptr: int, t0: float, h: float, n_steps: int, w, comps: ComponentTable,
+                params: NewtonParams | None = None, checkpoint_every: int = 50,
+                krylov: BiCgStabParams | None = None):
+        """do/dp of o = w . x(t0 + n_steps h) for every resistor, capacitor and
+        diode Is (the DC start x0 included).  x0 is left unchanged.
+        Returns (dict of gradients, info)."""
+        p, keep = (params or NewtonParams()).to_c()
+        kp = (krylov or BiCgStabParams(max_iterations=20000, tolerance=1e-14)).to_c()
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        gr = np.zeros(len(comps.r_ohms))
+        gc = np.zeros(len(comps.c_farads))
+        gd = np.zeros(len(self.plan.sysm.diode_descriptors))
+        info = _lib.AdjointInfo()
+        cc = comps.to_c()
+        st = self.ctx.lib.ohm_transient_adjoint(self._h, C.c_void_p(int(x0_dev_ptr)), float(t0), float(h),
+                                                int(n_steps), int(checkpoint_every), C.byref(p), dptr(w),
+                                                C.byref(cc), C.byref(kp), dptr(gr) if len(gr) else None,
+                                                dptr(gc) if len(gc) else None, dptr(gd) if len(gd) else None,
+                                                C.byref(info))
+        del keep
+        if st != _lib.OK:
+            _raise(st)
+        return {"R": gr, "C": gc, "Is": gd}, info.as_dict()
 
     def run(self, x_dev_ptr: int, t0: float, h: float, n_steps: int, params: NewtonParams | None = None,
             steps_per_launch: int = 100, graph: bool = True, check: bool = True):

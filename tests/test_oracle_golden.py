@@ -393,3 +393,45 @@ def test_ac_frequency_grid(grid):
     from oracle import ac_ref
     from ohmnivore_b200 import solver as S
     np.testing.assert_array_equal(S.ac_frequencies(*grid), np.array(ac_ref.generate_frequencies(*grid)))
+
+
+# ---- adjoint oracle: LU adjoint = forward sensitivity = central finite differences ----
+def _fd_output(ckt, mutate, h, n_steps, probe_label):
+    """o = V(probe) after n_steps BE steps from the DC point, for a circuit
+    changed by `mutate(ckt_copy, sysm)` (returns the new system)."""
+    from oracle import newton_ref
+    s = mutate()
+    x0, _ = newton_ref.newton(s)
+    states = __import__("oracle.adjoint_ref", fromlist=["x"]).transient_states(s, x0, 0.0, h, n_steps)
+    return states[-1][s.node_index(probe_label)]
+
+
+def test_adjoint_oracle_agrees_with_forward_sensitivity_and_fd():
+    import copy
+    from oracle import adjoint_ref, newton_ref
+    from ohmnivore_b200 import solver as S
+    ckt = ck.rc_diode_mesh(4, 4, seed=4, diode_frac=0.25)
+    s = mna.compile_circuit(ckt)
+    comps = S.ComponentTable(ckt, s)
+    h, n_steps = 2e-12, 12
+    probe = 2 + 15                                  # opposite corner of the 4x4 mesh
+    x0, _ = newton_ref.newton(s)
+    states = adjoint_ref.transient_states(s, x0, 0.0, h, n_steps)
+    w = np.zeros(s.size)
+    w[s.node_index(probe)] = 1.0
+    g = adjoint_ref.transient_adjoint(s, comps, states, h, w)
+    rel = lambda a, b: abs(a - b) / max(abs(b), 1e-300)  # noqa: E731
+    for kind, j in (("R", 3), ("R", 11), ("C", 5), ("C", 15), ("Is", 0)):
+        fs = adjoint_ref.forward_sensitivity(s, comps, states, h, w, kind, j)
+        assert rel(g[kind][j], fs) < 1e-8, (kind, j)
+    # central differences, relative step 1e-6, on R and C
+    for kind, idx in (("R", comps.r_index[3]), ("C", comps.c_index[5])):
+        v = ckt.value[idx]
+        outs = []
+        for sign in (1, -1):
+            c2 = copy.deepcopy(ckt)
+            c2.value[idx] = v * (1 + sign * 1e-6)
+            outs.append(_fd_output(c2, lambda c2=c2: mna.compile_circuit(c2), h, n_steps, probe))
+        fd = (outs[0] - outs[1]) / (2e-6 * v)
+        j = 3 if kind == "R" else 5
+        assert rel(g[kind][j], fd) < 1e-6, (kind, g[kind][j], fd)
