@@ -363,7 +363,9 @@ ohm_status ohm_transient_run(ohm_transient *tr, double *x_inout_device, double t
  * step back-stamps as above plus capacitor (a, b, C):
  * -(lambda_a - lambda_b)((v_a - v_b)_n - (v_a - v_b)_{n-1}) / h.  The forward
  * states are recomputed segment by segment from checkpoints taken every
- * `checkpoint_every` steps.  Gradients accumulate in FP64 on the device. */
+ * `checkpoint_every` steps.  Gradients accumulate in FP64 on the device.
+ * When x_0 is identically zero (all sources off at t0) every DC term is zero
+ * and the DC start solve is skipped (info->linear_solves = n_steps). */
 typedef struct {
     int64_t n_resistors;
     const int32_t *r_a, *r_b;    /* system rows of the terminals, -1 = ground */

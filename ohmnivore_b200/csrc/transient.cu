@@ -796,15 +796,29 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
             const double *xp = s == s0 ? ck + (size_t)sg * n : S + (size_t)(s - s0 - 1) * n;
             st = A.step(t->plan, xn, xp, t->aval, inv_h, kp, kiters);
             ++solves;
-            if (st != OHM_OK) break;
+            if (st != OHM_OK) {
+                st = ohm_fail(st, "adjoint solve of step %d: %s", s, ohm_last_error());
+                break;
+            }
             ct_rhs_kernel<<<steps_grid(n), 256, 0, c->stream>>>(A.rhs, d_ctrp, d_ctcol, d_ctval, A.lam, inv_h, n);
             CUDA_TRY(cudaGetLastError());
         }
     }
     // ---- the DC start: J_0^T lambda_0 = (C/h)^T lambda_1 ----
+    // Every DC back-stamp term carries a terminal voltage difference or
+    // exp(v/nVt) - 1 at x_0, so when x_0 is zero the whole term is zero and
+    // the solve is skipped.
+    bool x0_zero = false;
     if (st == OHM_OK) {
+        std::vector<double> hx(n);
+        CUDA_TRY(cudaMemcpyAsync(hx.data(), ck, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        x0_zero = std::all_of(hx.begin(), hx.end(), [](double v) { return v == 0.0; });
+    }
+    if (st == OHM_OK && !x0_zero) {
         st = A.step(t->plan, ck, nullptr, nullptr, 0.0, kp, kiters);
         ++solves;
+        if (st != OHM_OK) st = ohm_fail(st, "adjoint solve of the DC start: %s", ohm_last_error());
     }
     restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
     if (st == OHM_OK) st = A.download(d_out_dr, d_out_dc, d_out_dis, nullptr);
