@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--tran-stages", type=int, default=100_000,
                    help="inverter-chain stages of the transient measurement (0 skips it)")
     p.add_argument("--tran-steps", type=int, default=2000)
+    p.add_argument("--adjoint-rows", type=int, default=1000,
+                   help="RC-diode mesh size of the adjoint measurement (0 skips it)")
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                    help="one warm-up and one timed solve only (for an ncu capture)")
     return p.parse_args()
@@ -358,6 +360,8 @@ def main():
         line["batch"] = batch_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if args.tran_stages > 0:
         line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+    if args.adjoint_rows > 0:
+        line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -544,6 +548,103 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
             "dc_start": float(np.max(np.abs(xd[:sysm.n_nodes] - ref_dc[:sysm.n_nodes])) / 1.8)}
         res["cpu_baseline"] = {"value": k / cpu_s, "unit": "timesteps/s", "cores": 1, "kind": "port",
                                "sample": f"{k} BE steps of the same chain, LU Newton per step, single thread"}
+    tr.close()
+    plan.close()
+    return res
+
+
+def adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """Adjoint sensitivities on the 1000x1000 RC mesh with diodes at 5% of the
+    nodes (seed 4), driven by a 1 V step through 50 ohm: the gradient of one
+    node voltage at t = 1 ns (500 BE steps of 2 ps) w.r.t. every R, C and Is,
+    by the checkpointed transient adjoint (checkpoints every 50 steps, DC
+    start included).  Outputs: the corner opposite the drive (the configured
+    one) and node (10, 10) near the drive, where the response is nonzero;
+    GPU central differences (relative step 1e-6) on the three resistors with
+    the largest gradients of the latter."""
+    import copy
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    rows, nsteps, h = args.adjoint_rows, 500, 2e-12
+    ckt = circuits.rc_diode_mesh(rows, rows, seed=4)
+    sysm = mna.compile_circuit(ckt)
+    comps = S.ComponentTable(ckt, sysm)
+    pn = S.NewtonParams(max_iterations=100, abs_tol=1e-10, bicgstab_max_iterations=20000,
+                        bicgstab_tolerance=1e-14, inner_rtol=1e-6)
+    plan = S.NewtonPlan(sysm, ctx)
+    x = torch.zeros(sysm.size, dtype=torch.float64, device=f"cuda:{local_rank}")
+    plan.newton_device(x.data_ptr(), pn)
+    far = sysm.node_index(2 + rows * rows - 1)
+    near = sysm.node_index(2 + 10 * rows + 10)
+    tr = S.Transient(plan, [far, near])
+
+    def ev_time(fn):
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        r = fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        barrier()
+        return e0.elapsed_time(e1), r
+
+    xs = x.clone()
+    fwd_ms, wave = ev_time(lambda: tr.run(xs.data_ptr(), 0.0, h, nsteps, pn, steps_per_launch=100))
+    res = {"workload": f"RC mesh {rows}x{rows} with diodes at 5% of nodes, {sysm.size} unknowns, "
+                       f"{len(comps.r_ohms)} R + {len(comps.c_farads)} C + {len(sysm.diode_descriptors)} Is "
+                       f"parameters, {nsteps} BE steps of 2 ps",
+           "forward_ms": fwd_ms, "unit": "gradients/s"}
+    out = {}
+    for name, row in (("opposite_corner", far), ("node_10_10", near)):
+        w = np.zeros(sysm.size)
+        w[row] = 1.0
+        with ClockSampler(local_rank) as clk:
+            ms, (g, info) = ev_time(lambda: tr.adjoint(x.data_ptr(), 0.0, h, nsteps, w, comps, pn, 50))
+        out[name] = {"output_V": info["output"], "adjoint_ms": ms, "linear_solves": info["linear_solves"],
+                     "krylov_iterations": info["krylov_iterations"],
+                     "max_abs_grad": {k: float(np.max(np.abs(v))) for k, v in g.items()},
+                     "nonzero_grads": {k: int(np.count_nonzero(v)) for k, v in g.items()},
+                     "clocks": clk.summary()}
+        if name == "node_10_10":
+            fd_err = []
+            for j in np.argsort(-np.abs(g["R"]))[:3]:
+                idx = comps.r_index[j]
+                v = ckt.value[idx]
+                outs = []
+                for sign in (1, -1):
+                    c2 = copy.deepcopy(ckt)
+                    c2.value[idx] = v * (1 + sign * 1e-6)
+                    s2 = mna.compile_circuit(c2)
+                    p2 = S.NewtonPlan(s2, ctx)
+                    t2 = S.Transient(p2, [near])
+                    x2 = torch.zeros(s2.size, dtype=torch.float64, device=x.device)
+                    p2.newton_device(x2.data_ptr(), pn)
+                    outs.append(t2.run(x2.data_ptr(), 0.0, h, nsteps, pn, steps_per_launch=100)[-1, 0])
+                    t2.close()
+                    p2.close()
+                fd = (outs[0] - outs[1]) / (2e-6 * v)
+                fd_err.append(abs(g["R"][j] - fd) / abs(fd))
+            out[name]["rel_err_vs_central_differences"] = {"resistors": 3, "max": float(max(fd_err))}
+    res.update(out)
+    res["value"] = world * 1000.0 / out["node_10_10"]["adjoint_ms"]
+    if rank == 0 and not args.no_cpu_baseline:
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+        from oracle import adjoint_ref, transient_ref
+        xh = x.cpu().numpy()
+        t0 = time.perf_counter()
+        A = transient_ref.companion(sysm, h)
+        J = adjoint_ref._jacobian(sysm, A, xh)
+        w = np.zeros(sysm.size)
+        w[near] = 1.0
+        lam = spl.splu(J.T.tocsc()).solve(w)
+        adjoint_ref.backstamp(sysm, comps, xh, xh, lam, h)
+        one = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": 1.0 / (one * (nsteps + 1)), "unit": "gradients/s", "cores": 1,
+                               "kind": "port", "sample": "1 reverse step (assemble J, LU of J^T, back-stamp) "
+                                                         f"timed and scaled to {nsteps + 1} solves, no forward pass"}
     tr.close()
     plan.close()
     return res
