@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--tran-steps", type=int, default=2000)
     p.add_argument("--adjoint-rows", type=int, default=1000,
                    help="RC-diode mesh size of the adjoint measurement (0 skips it)")
+    p.add_argument("--sections", default="dc,batch,transient,adjoint",
+                   help="comma list of dc (the headline), batch, transient, adjoint; a run without dc "
+                        "prints only the chosen sections (for profiling small cases)")
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                    help="one warm-up and one timed solve only (for an ncu capture)")
     return p.parse_args()
@@ -223,6 +226,23 @@ def main():
         if world > 1:
             dist.barrier()
 
+    sections = set(args.sections.split(","))
+    if "dc" not in sections:
+        line = {"metric": METRIC, "sections_only": sorted(sections)}
+        if "batch" in sections and args.batch > 0:
+            line["batch"] = batch_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "transient" in sections and args.tran_stages > 0:
+            line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "adjoint" in sections and args.adjoint_rows > 0:
+            line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        plan.close()
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     def timed_solves(mixed, steps, warmup):
         params = newton_params(mixed)
         infos = []
@@ -356,11 +376,11 @@ def main():
         line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
                                 "sample": f"1 full DC solve of the workload ({it_ref} FP64 Newton "
                                           "iterations, SuperLU per iteration), single thread"}
-    if args.batch > 0:
+    if "batch" in sections and args.batch > 0:
         line["batch"] = batch_section(args, S, ctx, stream, barrier, world, rank, local_rank)
-    if args.tran_stages > 0:
+    if "transient" in sections and args.tran_stages > 0:
         line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
-    if args.adjoint_rows > 0:
+    if "adjoint" in sections and args.adjoint_rows > 0:
         line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
