@@ -369,7 +369,7 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
         }
     }
     cudaStreamSynchronize(c->stream);
-    for (void *q : allocs) cudaFree(q);
+    for (void *q : allocs) ohm_pool_free(q);
     if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "AC sweep: %s", cudaGetErrorString(e));
     if (failed >= 0)
         return ohm_fail(OHM_ERR_SOLVE, "BiCGSTAB did not converge at frequency point %lld (%.6e Hz, code %d)",

@@ -99,12 +99,14 @@ extern "C" ohm_status ohm_ctx_create(int device, ohm_ctx **out) {
 static void ctx_free(ohm_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    cudaFree(c->sync_words);
-    cudaFree(c->info_dev);
+    ohm_pool_free(c->sync_words);
+    ohm_pool_free(c->info_dev);
     cudaFreeHost(c->info_host);
-    cudaFree(c->dot_scratch);
+    ohm_pool_free(c->dot_scratch);
     if (c->stream) cudaStreamDestroy(c->stream);
+    const int dev = c->device;
     delete c;
+    ohm_pool_trim(dev);            // cached blocks of this device go back to CUDA
 }
 
 extern "C" ohm_status ohm_ctx_destroy(ohm_ctx *c) {
@@ -259,8 +261,8 @@ struct Workspace {
     uint8_t *rowflag = nullptr;
     bool any_pair = false;
     void release() {
-        cudaFree(vec); cudaFree(r64); cudaFree(dx); cudaFree(partials);
-        cudaFree(partner); cudaFree(diag_slot); cudaFree(off_slot); cudaFree(rowflag);
+        ohm_pool_free(vec); ohm_pool_free(r64); ohm_pool_free(dx); ohm_pool_free(partials);
+        ohm_pool_free(partner); ohm_pool_free(diag_slot); ohm_pool_free(off_slot); ohm_pool_free(rowflag);
         vec = r64 = dx = partials = nullptr; partner = nullptr; diag_slot = off_slot = nullptr;
         rowflag = nullptr;
     }
@@ -312,7 +314,7 @@ struct IsaiDev {
     void release() {
         void *ptrs[] = {aug_rp, aug_col, aug_diag, cp_ptr, cp_pair, aug_map, f0, f1, ml_val, mu_val,
                         ml_rp, ml_col, ml_cp, ml_row, ml_pos, mu_rp, mu_col, mu_cp, mu_row, mu_pos};
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) ohm_pool_free(p);
         *this = IsaiDev{};
     }
     template <typename T>
@@ -402,7 +404,7 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     ohm_status st = OHM_OK;
     cudaError_t e = ws.alloc(n, c->num_sms);
     if (e == cudaSuccess && mixed) e = dalloc(&v32, nnz);
-    if (e != cudaSuccess) { ws.release(); cudaFree(v32); return fail(OHM_ERR_CUDA, "workspace: %s", cudaGetErrorString(e)); }
+    if (e != cudaSuccess) { ws.release(); ohm_pool_free(v32); return fail(OHM_ERR_CUDA, "workspace: %s", cudaGetErrorString(e)); }
     PcHost pc;
     build_precond(n, h_rp, h_col, h_val, {}, p->precond == OHM_PRECOND_AUTO, pc);
     e = ws.upload_pc(pc, c->stream);
@@ -413,7 +415,7 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
         e = cudaGetLastError();
         ++launches;
     }
-    if (e != cudaSuccess) { ws.release(); cudaFree(v32); return fail(OHM_ERR_CUDA, "setup: %s", cudaGetErrorString(e)); }
+    if (e != cudaSuccess) { ws.release(); ohm_pool_free(v32); return fail(OHM_ERR_CUDA, "setup: %s", cudaGetErrorString(e)); }
     KernelArgs a{};
     a.n = (int)n; a.nnz = (int)nnz;
     a.row_ptr = d_rp; a.col = d_col; a.vals64 = d_val; a.vals32 = v32;
@@ -436,7 +438,7 @@ static ohm_status solve_real_impl(ohm_ctx *c, int64_t n, int64_t nnz, const uint
     cudaStreamSynchronize(c->stream);
     ws.release();
     isai.release();
-    cudaFree(v32);
+    ohm_pool_free(v32);
     return st;
 }
 
@@ -471,7 +473,7 @@ extern "C" ohm_status ohm_solve_real(ohm_ctx *c, int64_t n, int64_t nnz, const u
         if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "download: %s", cudaGetErrorString(e));
     }
     cudaStreamSynchronize(c->stream);
-    cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_b); cudaFree(d_x);
+    ohm_pool_free(d_rp); ohm_pool_free(d_col); ohm_pool_free(d_val); ohm_pool_free(d_b); ohm_pool_free(d_x);
     return st;
 }
 
@@ -515,19 +517,19 @@ struct ohm_plan {
 
 static void plan_free(ohm_plan *p) {
     if (!p) return;
-    cudaFree(p->rp); cudaFree(p->col); cudaFree(p->base_vals); cudaFree(p->vals64); cudaFree(p->base_b);
-    cudaFree(p->b); cudaFree(p->vals32); cudaFree(p->x_prev); cudaFree(p->x_scratch);
-    cudaFree(p->diodes); cudaFree(p->bjts); cudaFree(p->mosfets); cudaFree(p->vaf);
-    cudaFree(p->mstamp); cudaFree(p->rstamp);
-    cudaFree(p->mslot); cudaFree(p->mslot_ptr); cudaFree(p->mslot_ids);
-    cudaFree(p->rrow); cudaFree(p->rrow_ptr); cudaFree(p->rrow_ids);
-    cudaFree(p->node_scale);
-    cudaFree(p->stampflag); cudaFree(p->x_good);
+    ohm_pool_free(p->rp); ohm_pool_free(p->col); ohm_pool_free(p->base_vals); ohm_pool_free(p->vals64); ohm_pool_free(p->base_b);
+    ohm_pool_free(p->b); ohm_pool_free(p->vals32); ohm_pool_free(p->x_prev); ohm_pool_free(p->x_scratch);
+    ohm_pool_free(p->diodes); ohm_pool_free(p->bjts); ohm_pool_free(p->mosfets); ohm_pool_free(p->vaf);
+    ohm_pool_free(p->mstamp); ohm_pool_free(p->rstamp);
+    ohm_pool_free(p->mslot); ohm_pool_free(p->mslot_ptr); ohm_pool_free(p->mslot_ids);
+    ohm_pool_free(p->rrow); ohm_pool_free(p->rrow_ptr); ohm_pool_free(p->rrow_ids);
+    ohm_pool_free(p->node_scale);
+    ohm_pool_free(p->stampflag); ohm_pool_free(p->x_good);
     void *lp[] = {p->longflag, p->lseg_flag, p->long_row, p->long_chunk_ptr, p->long_chunk_owner, p->long_chunk_beg,
                   p->long_chunk_end, p->lseg, p->lseg_chunk_ptr, p->lseg_chunk_owner, p->lseg_chunk_beg,
                   p->lseg_chunk_end, p->long_part, p->lseg_part};
-    for (void *q : lp) cudaFree(q);
-    cudaFree(p->trace);
+    for (void *q : lp) ohm_pool_free(q);
+    ohm_pool_free(p->trace);
     p->ws.release();
     p->isai.release();
     delete p;
@@ -882,7 +884,7 @@ extern "C" ohm_status ohm_isai_apply(ohm_ctx *c, int64_t n, int64_t nnz, const u
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) st = fail(OHM_ERR_CUDA, "isai apply: %s", cudaGetErrorString(e));
     cudaStreamSynchronize(c->stream);
-    cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_r); cudaFree(d_z); cudaFree(d_y);
+    ohm_pool_free(d_rp); ohm_pool_free(d_col); ohm_pool_free(d_val); ohm_pool_free(d_r); ohm_pool_free(d_z); ohm_pool_free(d_y);
     isai.release();
     return st;
 }
@@ -1078,8 +1080,8 @@ ohm_status ohm_linsys_solve(ohm_linsys *L, double *d_vals, double *d_b, double *
 void ohm_linsys_destroy(ohm_linsys *L) {
     if (!L) return;
     cudaStreamSynchronize(L->ctx->stream);
-    cudaFree(L->rp);
-    cudaFree(L->col);
+    ohm_pool_free(L->rp);
+    ohm_pool_free(L->col);
     L->ws.release();
     delete L;
 }

@@ -71,7 +71,7 @@ extern "C" ohm_status ohm_buf_create(ohm_ctx *c, int64_t n, ohm_buf **out) {
     cudaError_t e = dalloc(&b->d, n);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d, 0, std::max<int64_t>(n, 1) * sizeof(double), c->stream);
     if (e != cudaSuccess) {
-        cudaFree(b->d);
+        ohm_pool_free(b->d);
         delete b;
         return ohm_fail(OHM_ERR_CUDA, "buffer allocation: %s", cudaGetErrorString(e));
     }
@@ -85,7 +85,7 @@ extern "C" ohm_status ohm_buf_destroy(ohm_buf *b) {
     ohm_ctx *c = b->ctx;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    cudaFree(b->d);
+    ohm_pool_free(b->d);
     delete b;
     ohm_ctx_release(c);
     return OHM_OK;
@@ -129,7 +129,7 @@ extern "C" ohm_status ohm_csr_upload(ohm_ctx *c, int64_t n, int64_t nnz, const u
     if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(m->val, values, nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-        cudaFree(m->rp); cudaFree(m->col); cudaFree(m->val);
+        ohm_pool_free(m->rp); ohm_pool_free(m->col); ohm_pool_free(m->val);
         delete m;
         return ohm_fail(OHM_ERR_CUDA, "CSR upload: %s", cudaGetErrorString(e));
     }
@@ -151,7 +151,7 @@ extern "C" ohm_status ohm_csr_destroy(ohm_csr *m) {
     ohm_ctx *c = m->ctx;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    cudaFree(m->rp); cudaFree(m->col); cudaFree(m->val);
+    ohm_pool_free(m->rp); ohm_pool_free(m->col); ohm_pool_free(m->val);
     delete m;
     ohm_ctx_release(c);
     return OHM_OK;

@@ -204,7 +204,7 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     if (e == cudaSuccess && nnz) e = ohm_f64_to_f32(a.vals64, v32, nnz, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);   // host vectors go out of scope
     if (e != cudaSuccess) {
-        for (void *p : b->allocs) cudaFree(p);
+        for (void *p : b->allocs) ohm_pool_free(p);
         delete b;
         return ohm_fail(OHM_ERR_CUDA, "batch upload: %s", cudaGetErrorString(e));
     }
@@ -222,7 +222,7 @@ extern "C" ohm_status ohm_batch_destroy(ohm_batch *b) {
     ohm_ctx *c = b->ctx;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (void *p : b->allocs) cudaFree(p);
+    for (void *p : b->allocs) ohm_pool_free(p);
     delete b;
     ohm_ctx_release(c);
     return OHM_OK;

@@ -86,10 +86,17 @@ struct ohm_csr {
     double *val;
 };
 
+// Device memory of the library's buffers comes from a per-device cache
+// (pool.cu).  Every buffer is released with ohm_pool_free after the work on
+// it has completed (the owner synchronises its stream first).
+cudaError_t ohm_pool_alloc(void **p, size_t bytes);
+void ohm_pool_free(void *p);
+void ohm_pool_trim(int device);
+
 template <typename T>
 inline cudaError_t dalloc(T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
-    return cudaMalloc((void **)p, count * sizeof(T));
+    return ohm_pool_alloc((void **)p, count * sizeof(T));
 }
 

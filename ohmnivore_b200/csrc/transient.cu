@@ -310,7 +310,7 @@ extern "C" ohm_status ohm_transient_create(ohm_plan *plan, int64_t c_nnz, const 
     if (e == cudaSuccess) e = t->put(&t->st, (const TranDev *)nullptr, 1);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-        for (void *q : t->allocs) cudaFree(q);
+        for (void *q : t->allocs) ohm_pool_free(q);
         delete t;
         return ohm_fail(OHM_ERR_CUDA, "transient upload: %s", cudaGetErrorString(e));
     }
@@ -324,8 +324,8 @@ extern "C" ohm_status ohm_transient_destroy(ohm_transient *t) {
     ohm_ctx *c = t->ctx;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (void *q : t->allocs) cudaFree(q);
-    cudaFree(t->wave);
+    for (void *q : t->allocs) ohm_pool_free(q);
+    ohm_pool_free(t->wave);
     delete t;
     ohm_ctx_release(c);
     return OHM_OK;
@@ -421,7 +421,7 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
         CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     const int64_t need = (int64_t)n_steps * t->n_probes;
     if (need > t->wave_cap) {
-        cudaFree(t->wave);
+        ohm_pool_free(t->wave);
         t->wave = nullptr;
         t->wave_cap = 0;
         CUDA_TRY(dalloc(&t->wave, (size_t)need));
@@ -577,7 +577,7 @@ struct AdjointCtx {
     ~AdjointCtx() {
         if (c) cudaStreamSynchronize(c->stream);
         ohm_linsys_destroy(L);
-        for (void *p : allocs) cudaFree(p);
+        for (void *p : allocs) ohm_pool_free(p);
     }
     template <typename T>
     cudaError_t put(T **dst, const T *h, size_t count) {

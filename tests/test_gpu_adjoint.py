@@ -88,7 +88,8 @@ def test_transient_adjoint_matches_oracle_and_forward_sensitivity():
     for k in ("R", "C", "Is"):
         assert _rel(g[k], ref[k]) < 1e-8, k
     assert info["output"] == pytest.approx(states[-1][s.node_index(probe)], rel=1e-10)
-    assert info["steps"] == n_steps and info["linear_solves"] == n_steps + 1
+    # the DC start solve is skipped when x0 is zero (every DC term vanishes)
+    assert info["steps"] == n_steps and info["linear_solves"] == n_steps + (1 if np.any(x0) else 0)
     assert info["recompute_launches"] == 5                     # ceil(30 / 7) segments
     for kind, j in (("R", 4), ("C", 9), ("Is", 2)):
         fs = adjoint_ref.forward_sensitivity(s, comps, states, H, w, kind, j)
