@@ -141,7 +141,7 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     b->ctx = c;
     b->n_inst = n_inst; b->rows = rows; b->nnz = nnz; b->nd = nd; b->nq = nq; b->nm = nm;
     const double avg = (double)nnz / (double)rows;
-    b->lpr = avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : 8));
+    b->lpr = avg <= 5.5 ? 1 : (avg <= 12.0 ? 4 : 8);
     KernelArgs &a = b->args.base;
     a = KernelArgs{};
     uint32_t *u32 = nullptr;

@@ -919,7 +919,9 @@ __device__ __forceinline__ int cont_cap(const KernelArgs &a, int reference_cap) 
 // 0.1, 1000x drops, 10x subdivisions from the last good level, at most 13),
 // a solve at the true GMIN, then pseudo-transient continuation from the last
 // GMIN point (:331-490: alpha from 0.1, 100x drops, at most 7 subdivisions,
-// b += alpha x_good on node rows) and a final true-DC solve.  The reference's
+// b += alpha x_good on node rows) and a final true-DC solve.  The final
+// solves take the reference's own Newton limits (50 after GMIN stepping, 25
+// after pseudo-transient), the direct attempt the caller's.  The reference's
 // CPU sparse-LU retries have no counterpart.  The stages form a state machine
 // around one newton_run call site.  The leader writes `*info`; a false
 // return means a grid barrier gave up.
@@ -994,8 +996,8 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 if (target > 1e-13) {
                     c = RunCfg{target, 1.0, 0.0, 15, cont_cap(a, 300), false};
                 } else {
-                    stage = kGminFinal;
-                    c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+                    stage = kGminFinal;       // NewtonParams::default(): 50 iterations (dc.rs:255-262)
+                    c = RunCfg{0.0, 1.0, 0.0, 50, a.max_krylov, false};
                 }
                 break;
             case kGminFinal:
@@ -1018,8 +1020,8 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 if (target > 1e-8) {
                     c = RunCfg{target, 1.0, target, 20, cont_cap(a, 500), false};
                 } else {
-                    stage = kPseudoFinal;
-                    c = RunCfg{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+                    stage = kPseudoFinal;     // 25 iterations (dc.rs:449-454)
+                    c = RunCfg{0.0, 1.0, 0.0, 25, a.max_krylov, false};
                 }
                 break;
             default:

@@ -199,7 +199,7 @@ int steps_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((
 
 int tran_lpr(int64_t n, int64_t nnz) {
     const double avg = n > 0 ? (double)nnz / (double)n : 1.0;
-    return avg <= 2.5 ? 1 : (avg <= 5.5 ? 2 : (avg <= 12.0 ? 4 : 8));
+    return avg <= 5.5 ? 1 : (avg <= 12.0 ? 4 : 8);
 }
 
 }  // namespace
