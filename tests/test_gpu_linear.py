@@ -123,6 +123,48 @@ def test_mixed_precision_iterative_refinement(ctx):
     assert solver.last_info["final_residual_norm"] < 1e-14 * solver.last_info["b_norm"]
 
 
+@pytest.mark.parametrize("lengths", ["short", "mixed_long", "dense_rows"])
+def test_spmv_tile_and_fallback_paths(ctx, lengths):
+    """The backend SpMV is bit-identical to a sequential CSR product: short
+    rows take the 32-row tiles, tiles with more than 384 nonzeros (and rows
+    averaging over 16) fall back to a warp per row; empty rows give 0."""
+    rng = np.random.default_rng({"short": 1, "mixed_long": 2, "dense_rows": 3}[lengths])
+    n = 5000
+    if lengths == "short":
+        cnt = rng.integers(0, 8, n)
+    elif lengths == "mixed_long":
+        cnt = rng.integers(0, 6, n)
+        cnt[rng.choice(n, 40, replace=False)] = rng.integers(200, 3000, 40)
+    else:
+        cnt = rng.integers(20, 60, n)
+    rp = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+    col = np.concatenate([np.sort(rng.choice(n, c, replace=False)) for c in cnt]).astype(np.int64)
+    val = rng.standard_normal(len(col))
+    a = mna.Csr(n, n, rp, col, val)
+    x = rng.standard_normal(n)
+    ref = np.zeros(n)
+    for i in range(n):                       # sequential CSR order
+        acc = 0.0
+        for k in range(rp[i], rp[i + 1]):
+            acc += val[k] * x[col[k]]
+        ref[i] = acc
+    be = S.SolverBackend(ctx)
+    A = be.upload_matrix(a)
+    bx, by = be.new_buffer(n), be.new_buffer(n)
+    bx.upload(x)
+    be.spmv(A, bx, by)
+    got = by.download()
+    if lengths == "dense_rows":              # warp-per-row reduction order
+        np.testing.assert_allclose(got, ref, rtol=1e-13, atol=1e-13)
+    else:
+        short = np.zeros(n, bool)
+        for t in range(0, n, 32):            # tiles within the shared-memory cap are exact
+            if rp[min(t + 32, n)] - rp[t] <= 384:
+                short[t:t + 32] = True
+        np.testing.assert_array_equal(got[short], ref[short])
+        np.testing.assert_allclose(got, ref, rtol=1e-13, atol=1e-13)
+
+
 def test_backend_ops(ctx):
     """SolverBackend ops (backend.rs:51-96) vs numpy."""
     s = mna.compile_circuit(ck.diode_mesh(20, 20, seed=3))
