@@ -18,79 +18,46 @@ constexpr int kOpsBlock = 256;
 
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + kOpsBlock - 1) / kOpsBlock, 148 * 8)); }
 
-// One warp per row.
-__global__ void spmv_warp_kernel(int n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                                 const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y) {
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
-        double acc = 0.0;
-        for (uint32_t k = rp[row] + lane; k < rp[row + 1]; k += 32) acc += val[k] * x[col[k]];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) y[row] = acc;
-    }
-}
-
-// Tiled CSR SpMV for short rows.  Each warp takes a tile of 32 consecutive
-// rows: the tile's nonzeros are read coalesced (lane-strided over the tile's
-// nnz range), their products val * x[col] staged in shared memory, then lane
-// i sums row i's products in CSR order (the same order as a sequential CSR
-// SpMV).  Tiles with more than kTileCap nonzeros fall back to a warp per row.
-constexpr int kTileCap = 384;
+// CSR SpMV, one thread per row: lane i of a warp sums row base + i in CSR
+// order (the order of a sequential CSR product).  Consecutive lanes read
+// consecutive rows, so a warp's column / value loads cover one contiguous
+// stretch of the arrays and every fetched sector is used through L1; with
+// 8 blocks of 256 threads per SM this streams at the HBM copy rate on short
+// rows.  Rows longer than kLongRow would stall their warp, so they are found
+// by a ballot and summed by the whole warp (lane-strided, xor tree); on a
+// matrix of long rows this is a warp per row.
+constexpr uint32_t kLongRow = 32;
 constexpr int kStreamBlock = 256;
 
-__global__ void __launch_bounds__(kStreamBlock) spmv_tile_kernel(int n, const uint32_t *__restrict__ rp,
-                                                                 const uint32_t *__restrict__ col,
-                                                                 const double *__restrict__ val,
-                                                                 const double *__restrict__ x,
-                                                                 double *__restrict__ y) {
-    __shared__ double prod[kStreamBlock / 32][kTileCap];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int ntiles = (n + 31) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    double *pw = prod[wib];
-    for (int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntiles; tile += nwarps) {
-        const int r0 = tile << 5;
-        const int rows = min(32, n - r0);
-        const uint32_t rb = lane < rows ? rp[r0 + lane] : 0u;
-        const uint32_t re = lane < rows ? rp[r0 + lane + 1] : 0u;
-        const uint32_t kb = __shfl_sync(0xffffffffu, rb, 0);
-        const uint32_t ke = __shfl_sync(0xffffffffu, re, rows - 1);
-        if (ke - kb <= (uint32_t)kTileCap) {
-            // all of this lane's column / value loads first, then all its
-            // gathers: up to kTileCap / 32 independent requests in flight
-            constexpr int U = kTileCap / 32;
-            uint32_t c[U];
-            double v[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t k = kb + lane + 32u * u;
-                c[u] = k < ke ? col[k] : 0u;
-                v[u] = k < ke ? val[k] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t k = kb + lane + 32u * u;
-                if (k < ke) pw[k - kb] = v[u] * x[c[u]];
-            }
-            __syncwarp();
-            if (lane < rows) {
-                double acc = 0.0;
-                for (uint32_t k = rb; k < re; ++k) acc += pw[k - kb];
-                y[r0 + lane] = acc;
-            }
-            __syncwarp();
-        } else {
-            for (int r = 0; r < rows; ++r) {
-                const uint32_t b = rp[r0 + r], e = rp[r0 + r + 1];
-                double acc = 0.0;
-                for (uint32_t k = b + lane; k < e; k += 32) acc += val[k] * x[col[k]];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) y[r0 + r] = acc;
-            }
+__global__ void __launch_bounds__(kStreamBlock) spmv_row_kernel(int n, const uint32_t *__restrict__ rp,
+                                                                const uint32_t *__restrict__ col,
+                                                                const double *__restrict__ val,
+                                                                const double *__restrict__ x,
+                                                                double *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int threads = gridDim.x * blockDim.x;
+    // warp-uniform loop bound: the warp's first row
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x - lane; base < n; base += threads) {
+        const int64_t row = base + lane;
+        uint32_t b = 0, e = 0;
+        if (row < n) {
+            b = rp[row];
+            e = rp[row + 1];
         }
+        const bool is_long = e - b > kLongRow;
+        double acc = 0.0;
+        if (!is_long)   // product and sum rounded separately, as a sequential CSR product does (no FMA)
+            for (uint32_t k = b; k < e; ++k) acc = __dadd_rn(acc, __dmul_rn(val[k], x[col[k]]));
+        for (unsigned pending = __ballot_sync(0xffffffffu, is_long); pending; pending &= pending - 1) {
+            const int src = __ffs(pending) - 1;
+            const uint32_t lb = __shfl_sync(0xffffffffu, b, src), le = __shfl_sync(0xffffffffu, e, src);
+            double part = 0.0;
+            for (uint32_t k = lb + lane; k < le; k += 32) part += val[k] * x[col[k]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (lane == src) acc = part;
+        }
+        if (row < n) y[row] = acc;
     }
 }
 
@@ -223,16 +190,9 @@ extern "C" ohm_status ohm_spmv(ohm_ctx *c, const ohm_csr *a, const ohm_buf *x, o
     if (!c || !a || !x || !y) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
     if (x->n != a->n || y->n != a->n) return ohm_fail(OHM_ERR_INVALID_ARG, "spmv dimension mismatch");
     if (a->n == 0) return OHM_OK;
-    const double avg = (double)a->nnz / (double)a->n;
-    if (avg <= 16.0) {
-        // tiles of 32 rows, one warp each; grid sized to the SMs' resident warps
-        const int64_t tiles = (a->n + 31) / 32;
-        const int grid = (int)std::min<int64_t>((tiles * 32 + kStreamBlock - 1) / kStreamBlock, 148 * 8);
-        spmv_tile_kernel<<<grid, kStreamBlock, 0, c->stream>>>((int)a->n, a->rp, a->col, a->val, x->d, y->d);
-    } else {
-        const int grid = (int)std::min<int64_t>((a->n * 32 + kOpsBlock - 1) / kOpsBlock, 148 * 16);
-        spmv_warp_kernel<<<grid, kOpsBlock, 0, c->stream>>>((int)a->n, a->rp, a->col, a->val, x->d, y->d);
-    }
+    // 8 resident blocks of 256 threads per SM, grid-stride over the rows
+    const int grid = (int)std::min<int64_t>((a->n + kStreamBlock - 1) / kStreamBlock, 148 * 8);
+    spmv_row_kernel<<<grid, kStreamBlock, 0, c->stream>>>((int)a->n, a->rp, a->col, a->val, x->d, y->d);
     CUDA_TRY(cudaGetLastError());
     return OHM_OK;
 }
