@@ -289,8 +289,9 @@ ohm_status ohm_ac_sweep(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *ro
  * is linear only: it forms A = G + C/h and b = b(t_n) + (C/h) x_{n-1} per BE
  * step (:285-333) and ignores nonlinear devices; this engine uses the same
  * companion system as the base of a Newton solve (device evaluation and
- * stamping on top of it) at every step.  Its adaptive BE/TRAP step control
- * (:84-178) is not implemented: the step is fixed.
+ * stamping on top of it) at every step.  ohm_transient_run takes fixed BE
+ * steps; ohm_transient_run_adaptive below is the reference's adaptive BE/TRAP
+ * step control (:84-178).
  *
  * Time-dependent sources (collect_source_info / evaluate_b_at_time,
  * transient.rs:212-280, and transient_source.rs:8-118): b(t) is the sum over
@@ -346,6 +347,45 @@ ohm_status ohm_transient_destroy(ohm_transient *tr);
 ohm_status ohm_transient_run(ohm_transient *tr, double *x_inout_device, double t0, double h, int32_t n_steps,
                              int32_t steps_per_launch, const ohm_newton_params *params, int32_t use_graph,
                              double *waveforms_host, ohm_transient_info *info);
+
+/* Adaptive BE / TRAP run of the reference's transient::run
+ * (src/analysis/transient.rs:77-178) from t = 0 to tstop: the first step and
+ * the step after a rejection are backward Euler; every other step solves
+ * the trapezoidal companion system (A = G + 2C/h, b = b(t_n) + (2C/h) x -
+ * f(x) + b(t_{n-1}), :336-352) and the BE one from the same x, estimates
+ * LTE = (2/3) max|x_trap - x_be| (:355-362) and accepts x_trap when
+ * LTE <= 1e-3, else retries with a smaller h; h_min = tstep / 10^4,
+ * h_max = tstep.  f(x) = G x + i(x): G x in the reference (linear
+ * circuits), plus the device currents here, where every solve is a Newton
+ * solve on the companion base.  x_inout_device holds x(0) and receives the
+ * last accepted x.  Output points: (0, x(0)) when tstart <= 0, then every
+ * accepted step with t >= tstart; the first max_points are written to
+ * times_host (max_points doubles) and waveforms_host (max_points x n_probes,
+ * row-major), either may be NULL; info->points counts them all, so a run
+ * with info->points > max_points was truncated and can be repeated with a
+ * larger capacity.  The whole run is one cooperative launch.  Errors:
+ * OHM_ERR_TIMESTEP as transient.rs:128-133, a failed Newton solve as in
+ * ohm_transient_run (info->failed_solve 1 = TRAP, 2 = BE). */
+typedef struct {
+    int32_t status;
+    int32_t accepted;            /* Stats::timesteps_accepted */
+    int32_t rejected;            /* Stats::timesteps_rejected */
+    int32_t points;              /* output points produced (kept: min(points, max_points)) */
+    int64_t newton_iterations;
+    int64_t krylov_iterations;
+    int32_t linear_solves;       /* companion solves: 1 per BE step, 2 per TRAP step (Stats::linear_solves) */
+    int32_t fp64_fallbacks;
+    int32_t krylov_code;
+    int32_t failed_solve;        /* 0 none, 1 TRAP, 2 BE */
+    double t_end;                /* time reached */
+    double h_last;               /* step size at the end */
+    double t_failed;             /* time of a failed solve (target) or of the timestep failure */
+    double max_residual;         /* max|dx| of the last Newton iteration of a failed solve */
+} ohm_adaptive_info;
+
+ohm_status ohm_transient_run_adaptive(ohm_transient *tr, double *x_inout_device, double tstep, double tstop,
+                                      double tstart, const ohm_newton_params *params, int32_t max_points,
+                                      double *times_host, double *waveforms_host, ohm_adaptive_info *info);
 
 /* ---------------------------------------------------------------- adjoint --
  * Sensitivities of one output o = w . x (w = do/dx, host, size n) with

@@ -58,6 +58,17 @@ class TransientInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AdaptiveInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("accepted", C.c_int32), ("rejected", C.c_int32), ("points", C.c_int32),
+                ("newton_iterations", C.c_int64), ("krylov_iterations", C.c_int64),
+                ("linear_solves", C.c_int32), ("fp64_fallbacks", C.c_int32), ("krylov_code", C.c_int32),
+                ("failed_solve", C.c_int32), ("t_end", C.c_double), ("h_last", C.c_double),
+                ("t_failed", C.c_double), ("max_residual", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # ohm_source (include/ohm.h), 104 bytes
 SOURCE_DTYPE = np.dtype([("kind", "<i4"), ("n_rows", "<i4"), ("rows", "<u4", (2,)), ("sign", "<f8", (2,)),
                          ("dc", "<f8"), ("p", "<f8", (7,)), ("pwl_offset", "<i4"), ("pwl_count", "<i4")],
@@ -143,6 +154,9 @@ SIGNATURES = {
                                _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                     C.POINTER(NewtonParamsC), C.c_int32, _dp, C.POINTER(TransientInfo)]),
+    "ohm_transient_run_adaptive": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double,
+                                             C.POINTER(NewtonParamsC), C.c_int32, _dp, _dp,
+                                             C.POINTER(AdaptiveInfo)]),
     "ohm_batch_autotune": (C.c_int, [_vp, C.POINTER(NewtonParamsC), C.c_int32, C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "ohm_batch_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),

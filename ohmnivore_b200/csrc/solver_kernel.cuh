@@ -610,6 +610,107 @@ struct RunOut {
     double last_dmax, bnorm_last, final_res;
 };
 
+// Device evaluation and stamping at a.x: every slot / rhs row touched by a
+// device becomes base + its contributions in canonical order (the stamp map;
+// slots and rows with many contributions are summed by warps in chunks
+// first), the rhs rows scaled by cfg.src; then the continuation terms when
+// a.continuation is set.  Untouched slots and rows are not written.  A false
+// return means a team sync gave up.
+template <class Team>
+__device__ __forceinline__ bool assemble(const KernelArgs &a, Team &g, const RunCfg &cfg,
+                                         const double *__restrict__ base_vals,
+                                         const double *__restrict__ base_b) {
+    const int gtid = g.gtid, gstride = g.gstride;
+    const int ndev = a.nd + a.nq + a.nm;
+    for (int k = gtid; k < ndev; k += gstride) {
+        if (k < a.nd) {
+            diode_stamps(a.diodes[k], a.x, a.mstamp + 4 * (size_t)k, a.rstamp + 2 * (size_t)k);
+        } else if (k < a.nd + a.nq) {
+            const int q = k - a.nd;
+            const double vaf = a.bjt_vaf ? a.bjt_vaf[q] : __longlong_as_double(0x7ff0000000000000LL);
+            bjt_stamps(a.bjts[q], vaf, a.x, a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)q,
+                       a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)q);
+        } else {
+            const int m = k - a.nd - a.nq;
+            mosfet_stamps(a.mosfets[m], a.x,
+                          a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)a.nq + 6 * (size_t)m,
+                          a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)a.nq + 2 * (size_t)m);
+        }
+    }
+    OHM_SYNC_OR(false);
+    // stamp map: each touched slot / row = base + contributions in canonical order;
+    // entries with many contributions are summed by warps in chunks first
+    if (a.n_lseg) {
+        const int lane = threadIdx.x & 31;
+        for (int c = gtid >> 5; c < a.n_lseg_chunks; c += gstride >> 5) {
+            const bool mat = (int)a.lseg[a.lseg_chunk_owner[c]] < a.n_mslots;
+            const uint32_t *ids = mat ? a.mslot_ids : a.rrow_ids;
+            const double *src = mat ? a.mstamp : a.rstamp;
+            double acc = 0.0;
+            for (uint32_t j = a.lseg_chunk_beg[c] + lane; j < a.lseg_chunk_end[c]; j += 32) acc += src[ids[j]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) a.lseg_part[c] = acc;
+        }
+        OHM_SYNC_OR(false);
+        for (int q = gtid >> 5; q < a.n_lseg; q += gstride >> 5) {
+            double acc = 0.0;
+            for (uint32_t c = a.lseg_chunk_ptr[q] + lane; c < a.lseg_chunk_ptr[q + 1]; c += 32)
+                acc += a.lseg_part[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                const int k = (int)a.lseg[q];
+                if (k < a.n_mslots) {
+                    const uint32_t slot = a.mslot[k];
+                    const double v = base_vals[slot] + acc;
+                    a.vals64[slot] = v;
+                    if (a.vals32) a.vals32[slot] = (float)v;
+                } else {
+                    const uint32_t row = a.rrow[k - a.n_mslots];
+                    a.b[row] = cfg.src * base_b[row] + acc;
+                }
+            }
+        }
+    }
+    for (int k = gtid; k < a.n_mslots + a.n_rrows; k += gstride) {
+        if (a.lseg_flag != nullptr && a.lseg_flag[k]) continue;
+        if (k < a.n_mslots) {
+            const uint32_t slot = a.mslot[k];
+            double acc = base_vals[slot];
+            for (uint32_t j = a.mslot_ptr[k]; j < a.mslot_ptr[k + 1]; ++j) acc += a.mstamp[a.mslot_ids[j]];
+            a.vals64[slot] = acc;
+            if (a.vals32) a.vals32[slot] = (float)acc;
+        } else {
+            const int q = k - a.n_mslots;
+            const uint32_t row = a.rrow[q];
+            double acc = cfg.src * base_b[row];
+            for (uint32_t j = a.rrow_ptr[q]; j < a.rrow_ptr[q + 1]; ++j) acc += a.rstamp[a.rrow_ids[j]];
+            a.b[row] = acc;
+        }
+    }
+    OHM_SYNC_OR(false);
+    if (a.continuation) {
+        // continuation terms on top of the assembled system; rows the
+        // stamp map does not write restart from their base values
+        for (int i = gtid; i < a.n; i += gstride) {
+            const uint8_t f = a.stampflag[i];
+            const bool node = i < a.n_nodes;
+            const uint32_t ds = a.diag_slot[i];
+            if (node && ds != kSentinel) {
+                const double v = ((f & 1) ? a.vals64[ds] : base_vals[ds]) + cfg.gshift;
+                a.vals64[ds] = v;
+                if (a.vals32) a.vals32[ds] = (float)v;
+            }
+            double bv = (f & 2) ? a.b[i] : cfg.src * base_b[i];
+            if (node && cfg.pt != 0.0) bv += cfg.pt * a.x_good[i];
+            a.b[i] = bv;
+        }
+        OHM_SYNC_OR(false);
+    }
+    return true;
+}
+
 // The Newton loop for one system, run by a team; results in `o` (identical in
 // every thread).  A false return means a grid barrier gave up.
 template <int LPR, class Team>
@@ -625,93 +726,7 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
     for (int outer = 0; outer < cfg.max_outer; ++outer) {
         // ---------------- device evaluation + stamping (Newton) ----------------
         if (a.newton) {
-            const int ndev = a.nd + a.nq + a.nm;
-            for (int k = gtid; k < ndev; k += gstride) {
-                if (k < a.nd) {
-                    diode_stamps(a.diodes[k], a.x, a.mstamp + 4 * (size_t)k, a.rstamp + 2 * (size_t)k);
-                } else if (k < a.nd + a.nq) {
-                    const int q = k - a.nd;
-                    const double vaf = a.bjt_vaf ? a.bjt_vaf[q] : __longlong_as_double(0x7ff0000000000000LL);
-                    bjt_stamps(a.bjts[q], vaf, a.x, a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)q,
-                               a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)q);
-                } else {
-                    const int m = k - a.nd - a.nq;
-                    mosfet_stamps(a.mosfets[m], a.x,
-                                  a.mstamp + 4 * (size_t)a.nd + 9 * (size_t)a.nq + 6 * (size_t)m,
-                                  a.rstamp + 2 * (size_t)a.nd + 3 * (size_t)a.nq + 2 * (size_t)m);
-                }
-            }
-            OHM_SYNC_OR(false);
-            // stamp map: each touched slot / row = base + contributions in canonical order;
-            // entries with many contributions are summed by warps in chunks first
-            if (a.n_lseg) {
-                const int lane = threadIdx.x & 31;
-                for (int c = gtid >> 5; c < a.n_lseg_chunks; c += gstride >> 5) {
-                    const bool mat = (int)a.lseg[a.lseg_chunk_owner[c]] < a.n_mslots;
-                    const uint32_t *ids = mat ? a.mslot_ids : a.rrow_ids;
-                    const double *src = mat ? a.mstamp : a.rstamp;
-                    double acc = 0.0;
-                    for (uint32_t j = a.lseg_chunk_beg[c] + lane; j < a.lseg_chunk_end[c]; j += 32) acc += src[ids[j]];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                    if (lane == 0) a.lseg_part[c] = acc;
-                }
-                OHM_SYNC_OR(false);
-                for (int q = gtid >> 5; q < a.n_lseg; q += gstride >> 5) {
-                    double acc = 0.0;
-                    for (uint32_t c = a.lseg_chunk_ptr[q] + lane; c < a.lseg_chunk_ptr[q + 1]; c += 32)
-                        acc += a.lseg_part[c];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                    if (lane == 0) {
-                        const int k = (int)a.lseg[q];
-                        if (k < a.n_mslots) {
-                            const uint32_t slot = a.mslot[k];
-                            const double v = a.base_vals[slot] + acc;
-                            a.vals64[slot] = v;
-                            if (a.vals32) a.vals32[slot] = (float)v;
-                        } else {
-                            const uint32_t row = a.rrow[k - a.n_mslots];
-                            a.b[row] = cfg.src * a.base_b[row] + acc;
-                        }
-                    }
-                }
-            }
-            for (int k = gtid; k < a.n_mslots + a.n_rrows; k += gstride) {
-                if (a.lseg_flag != nullptr && a.lseg_flag[k]) continue;
-                if (k < a.n_mslots) {
-                    const uint32_t slot = a.mslot[k];
-                    double acc = a.base_vals[slot];
-                    for (uint32_t j = a.mslot_ptr[k]; j < a.mslot_ptr[k + 1]; ++j) acc += a.mstamp[a.mslot_ids[j]];
-                    a.vals64[slot] = acc;
-                    if (a.vals32) a.vals32[slot] = (float)acc;
-                } else {
-                    const int q = k - a.n_mslots;
-                    const uint32_t row = a.rrow[q];
-                    double acc = cfg.src * a.base_b[row];
-                    for (uint32_t j = a.rrow_ptr[q]; j < a.rrow_ptr[q + 1]; ++j) acc += a.rstamp[a.rrow_ids[j]];
-                    a.b[row] = acc;
-                }
-            }
-            OHM_SYNC_OR(false);
-            if (a.continuation) {
-                // continuation terms on top of the assembled system; rows the
-                // stamp map does not write restart from their base values
-                for (int i = gtid; i < a.n; i += gstride) {
-                    const uint8_t f = a.stampflag[i];
-                    const bool node = i < a.n_nodes;
-                    const uint32_t ds = a.diag_slot[i];
-                    if (node && ds != kSentinel) {
-                        const double v = ((f & 1) ? a.vals64[ds] : a.base_vals[ds]) + cfg.gshift;
-                        a.vals64[ds] = v;
-                        if (a.vals32) a.vals32[ds] = (float)v;
-                    }
-                    double bv = (f & 2) ? a.b[i] : cfg.src * a.base_b[i];
-                    if (node && cfg.pt != 0.0) bv += cfg.pt * a.x_good[i];
-                    a.b[i] = bv;
-                }
-                OHM_SYNC_OR(false);
-            }
+            if (!assemble(a, g, cfg, a.base_vals, a.base_b)) return false;
         }
 
         // -------------------------- FP64 residual r64 = b - A x -------------------------

@@ -158,6 +158,217 @@ __global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a
     }
 }
 
+// Adaptive BE / TRAP step control of the reference (transient.rs:77-178):
+// the first step and the step after a rejection are BE; every other step
+// solves TRAP and BE from x_{n-1}, estimates LTE = (2/3) max|x_trap - x_be|
+// (compute_lte, :355-362), rejects it when LTE > 1e-3 (h *= clamp(0.9
+// sqrt(tol / LTE), 0.5, 2), at least h_min) and otherwise accepts x_trap and
+// takes h = clamp(h * that factor, h_min, h_max); h_min = tstep / 10^4,
+// h_max = tstep.  Companion matrices A = G + (alpha / h) C (:285-323) are
+// formed on the device for every solve.  TRAP's rhs is
+// b(t_n) + (2/h) C x_{n-1} - f(x_{n-1}) + b(t_{n-1}) (:336-352) with
+// f(x) = G x + i(x): the reference's G x_{n-1} plus, for nonlinear devices,
+// their currents, taken as J(x) x - b of the system stamped at x on the base
+// (G, 0), so TRAP integrates the same device equations Newton solves.
+constexpr int kAdTimestep = 20;   // consecutive rejections at h_min (OhmnivoreError::Timestep)
+
+struct AdaptDev {
+    int status, accepted, rejected, points;
+    long long newton_its, krylov_its;
+    int solves, fallbacks, kcode, failed_kind;
+    double t, h, t_fail, max_residual;
+};
+
+struct AdaptArgs {
+    double tstep, tstop, tstart;
+    int max_points;
+    long long nnz;
+    const double *g_vals;      // G, the plan's base values
+    const double *cg;          // C on G's pattern (0 off C)
+    const double *zeros;       // n zeros: the rhs base of the f(x) evaluation
+    double *aval;              // companion base values of the current solve
+    double *xs, *xt, *fdev;    // x_{n-1}, x_trap, f(x_{n-1})
+    double *times;             // output times (max_points)
+    AdaptDev *st;
+};
+
+template <int LPR>
+__global__ void __launch_bounds__(kSolverBlock, 1) adaptive_kernel(KernelArgs a, TranArgs T, AdaptArgs P) {
+    __shared__ double smem[32 * 4];
+    GridTeam g;
+    g.G = gridDim.x;
+    g.bid = blockIdx.x;
+    g.r0 = (int)(((long long)a.n * g.bid) / g.G);
+    g.r1 = (int)(((long long)a.n * (g.bid + 1)) / g.G);
+    g.gtid = g.bid * blockDim.x + threadIdx.x;
+    g.gstride = g.G * blockDim.x;
+    g.smem = smem;
+    g.partials = a.partials;
+    g.red = 0;
+    g.epoch = 0;
+    g.gs = a.gs;
+    const int r0 = g.r0, r1 = g.r1;
+    const double h_min = P.tstep / 10000.0, h_max = P.tstep, lte_tol = 1e-3;
+    constexpr int kMaxFailures = 10;
+    // every thread holds the same control state: it changes only through
+    // grid-wide results (Newton status, the all-reduced LTE)
+    double t = 0.0, h = fmin(P.tstep, h_max), t_next = 0.0, h_next = 0.0;
+    bool use_be = true;
+    int stage = 0;               // 0: new step, 1: its TRAP solve, 2: its BE solve
+    int fails = 0, points = 0, accepted = 0, rejected = 0, solves = 0, fallbacks = 0, kcode = 0;
+    int status = kOk, failed_kind = 0;
+    long long nits = 0, kits = 0;
+    double t_fail = 0.0, max_res = 0.0;
+
+    // output row `points` (kept only below max_points; the count continues)
+    auto record = [&](double tr) {
+        if (points < P.max_points) {
+            for (int k = g.gtid; k < T.n_probes; k += g.gstride)
+                T.wave[(size_t)points * T.n_probes + k] = a.x[T.probe[k]];
+            if (g.leader()) P.times[points] = tr;
+        }
+        ++points;
+    };
+    if (P.tstart <= 0.0) record(0.0);
+    while (true) {
+        if (stage == 0) {
+            if (!(t < P.tstop)) break;
+            if (t + h > P.tstop) h = P.tstop - t;
+            if (h < h_min * 0.5) break;
+            t_next = t + h;
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) P.xs[i] = a.x[i];
+            if (!use_be) {
+                // f(x_{n-1}) = J x - b of the system stamped at x on (G, 0)
+                for (long long k = g.gtid; k < P.nnz; k += g.gstride) {
+                    a.vals64[k] = P.g_vals[k];
+                    if (a.vals32) a.vals32[k] = (float)P.g_vals[k];
+                }
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.b[i] = 0.0;
+                if (!g.sync()) return;
+                const RunCfg c0{0.0, 1.0, 0.0, 0, 0, false};
+                if (!assemble(a, g, c0, P.g_vals, P.zeros)) return;
+                const double *xv = a.x;
+                auto x_at = [&](int j, bool) -> double { return xv[j]; };
+                auto f_row = [&](int i, double ax) { P.fdev[i] = ax - a.b[i]; };
+                spmv_rows<LPR, double>(a.row_ptr, a.col, a.vals64, (const uint8_t *)nullptr, r0, r1, x_at, f_row,
+                                       a.longflag);
+                if (!spmv_long<double>(a, g, a.col, a.vals64, (const uint8_t *)nullptr, x_at, f_row)) return;
+                if (!g.sync()) return;
+            }
+            stage = use_be ? 2 : 1;
+        }
+        // companion base A = G + (alpha / h) C and the step's rhs
+        const double fac = (stage == 1 ? 2.0 : 1.0) / h;
+        for (long long k = g.gtid; k < P.nnz; k += g.gstride) {
+            const double v = P.g_vals[k] + fac * P.cg[k];
+            P.aval[k] = v;
+            a.vals64[k] = v;
+            if (a.vals32) a.vals32[k] = (float)v;
+        }
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+            double bn = 0.0, bp = 0.0;
+            const int q = T.src_of_row[i];
+            if (q >= 0)
+                for (uint32_t e = T.srow_ptr[q]; e < T.srow_ptr[q + 1]; ++e) {
+                    const ohm_source &src = T.src[T.srow_src[e]];
+                    bn += T.srow_sign[e] * source_value(src, t_next, T.pwl);
+                    if (stage == 1) bp += T.srow_sign[e] * source_value(src, t, T.pwl);
+                }
+            double cx = 0.0;
+            for (uint32_t k = T.c_rp[i]; k < T.c_rp[i + 1]; ++k) cx += T.c_val[k] * a.x[T.c_col[k]];
+            const double bb = stage == 1 ? ((bn + fac * cx) - P.fdev[i]) + bp : bn + fac * cx;
+            T.beff[i] = bb;
+            a.b[i] = bb;
+        }
+        if (!g.sync()) return;
+        RunOut o;
+        const RunCfg c{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
+        if (!newton_run<LPR>(a, g, c, o)) return;
+        nits += o.outer_done;
+        kits += o.kiters;
+        fallbacks += o.fallbacks;
+        kcode = o.kcode;
+        ++solves;
+        if (o.status != kOk) {
+            status = o.status;
+            failed_kind = stage;
+            t_fail = t_next;
+            max_res = o.last_dmax;
+            break;
+        }
+        if (stage == 1) {            // keep x_trap, solve BE from x_{n-1}
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                P.xt[i] = a.x[i];
+                a.x[i] = P.xs[i];
+            }
+            if (!g.sync()) return;
+            stage = 2;
+            continue;
+        }
+        stage = 0;
+        if (!use_be) {
+            double mx[1] = {0.0};
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) mx[0] = fmax(mx[0], fabs(P.xt[i] - a.x[i]));
+            if (!g.template allmax<1>(mx)) return;
+            const double lte = (2.0 / 3.0) * mx[0];
+            const double factor = fmin(fmax(0.9 * sqrt(lte_tol / lte), 0.5), 2.0);
+            if (lte > lte_tol) {     // reject: smaller h, BE from x_{n-1}
+                h = fmax(h * factor, h_min);
+                ++fails;
+                if (fails >= kMaxFailures && h <= h_min * 1.01) {
+                    status = kAdTimestep;
+                    t_fail = t;
+                    break;
+                }
+                ++rejected;
+                use_be = true;
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = P.xs[i];
+                if (!g.sync()) return;
+                continue;
+            }
+            h_next = fmin(fmax(h * factor, h_min), h_max);
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = P.xt[i];
+            if (!g.sync()) return;
+        } else {
+            use_be = false;
+            h_next = h;
+        }
+        fails = 0;
+        ++accepted;
+        t = t_next;
+        h = h_next;
+        if (t >= P.tstart) record(t);
+    }
+    if (g.leader()) {
+        AdaptDev &d = *P.st;
+        d.status = status;
+        d.accepted = accepted;
+        d.rejected = rejected;
+        d.points = points;
+        d.newton_its = nits;
+        d.krylov_its = kits;
+        d.solves = solves;
+        d.fallbacks = fallbacks;
+        d.kcode = kcode;
+        d.failed_kind = failed_kind;
+        d.t = t;
+        d.h = h;
+        d.t_fail = t_fail;
+        d.max_residual = max_res;
+    }
+}
+
+using AdaptFn = void (*)(KernelArgs, TranArgs, AdaptArgs);
+
+AdaptFn pick_adaptive(int lpr) {
+    switch (lpr) {
+        case 1: return adaptive_kernel<1>;
+        case 2: return adaptive_kernel<2>;
+        case 4: return adaptive_kernel<4>;
+        default: return adaptive_kernel<8>;
+    }
+}
+
 using TranFn = void (*)(KernelArgs, TranArgs);
 
 TranFn pick_tran(int lpr) {
@@ -219,6 +430,12 @@ struct ohm_transient {
     TranDev *st = nullptr;
     double *wave = nullptr;
     int64_t wave_cap = 0;
+    // adaptive runs
+    double *cg = nullptr;                       // C on G's pattern (nnz)
+    double *ad_xs = nullptr, *ad_xt = nullptr, *ad_fdev = nullptr, *ad_zeros = nullptr;
+    AdaptDev *ad_st = nullptr;
+    double *times = nullptr;
+    int64_t times_cap = 0;
 
     template <typename T>
     cudaError_t put(T **dst, const T *h, size_t count) {
@@ -298,6 +515,11 @@ extern "C" ohm_status ohm_transient_create(ohm_plan *plan, int64_t c_nnz, const 
     if (e == cudaSuccess) e = t->put(&t->c_col, c_col, c_nnz);
     if (e == cudaSuccess) e = t->put(&t->c_val, c_values, c_nnz);
     if (e == cudaSuccess) e = t->put(&t->c_slot, slot.data(), c_nnz);
+    if (e == cudaSuccess) {
+        std::vector<double> cg(nnz, 0.0);
+        for (int64_t k = 0; k < c_nnz; ++k) cg[slot[k]] = c_values[k];
+        e = t->put(&t->cg, cg.data(), nnz);
+    }
     if (e == cudaSuccess) e = t->put(&t->aval, (const double *)nullptr, nnz);
     if (e == cudaSuccess) e = t->put(&t->beff, (const double *)nullptr, n);
     if (e == cudaSuccess) e = t->put(&t->pwl, pwl_points, 2 * (size_t)n_pwl_points);
@@ -326,49 +548,67 @@ extern "C" ohm_status ohm_transient_destroy(ohm_transient *t) {
     cudaStreamSynchronize(c->stream);
     for (void *q : t->allocs) ohm_pool_free(q);
     ohm_pool_free(t->wave);
+    ohm_pool_free(t->times);
     delete t;
     ohm_ctx_release(c);
     return OHM_OK;
 }
 
-// Kernel arguments of a run on x_dev with step h: the companion base
-// A = G + C/h is formed (and copied to the assembled arrays), the run
-// record zeroed.  Returns the kernel and grid to launch.
-static ohm_status tran_prepare(ohm_transient *t, double *x_dev, double h, const ohm_newton_params *np,
-                               KernelArgs &a, TranArgs &T, TranFn &fn, int &grid, const double *&G) {
+// Kernel arguments of a run on x_dev: the plan's system with the companion
+// base values t->aval and rhs base t->beff; G receives the plan's own base.
+static ohm_status tran_args(ohm_transient *t, double *x_dev, const ohm_newton_params *np, KernelArgs &a,
+                            TranArgs &T, const double *&G) {
     ohm_ctx *c = t->ctx;
     int64_t nnz = 0;
     ohm_status st = ohm_plan_kernel_args(t->plan, np, x_dev, a, &nnz);
     if (st != OHM_OK) return st;
     G = a.base_vals;
-    for (int phase = 0; phase < 3; ++phase) {
-        companion_kernel<<<steps_grid(phase == 1 ? t->c_nnz : nnz), 256, 0, c->stream>>>(
-            G, t->aval, a.vals64, a.vals32, nnz, t->c_slot, t->c_val, t->c_nnz, 1.0 / h, phase);
-        CUDA_TRY(cudaGetLastError());
-    }
-    CUDA_TRY(cudaMemsetAsync(t->st, 0, sizeof(TranDev), c->stream));
     a.base_vals = t->aval;
     a.base_b = t->beff;
     a.trace = nullptr;
     a.continuation = 0;
+    a.gs.count = (unsigned long long *)c->sync_words;
+    a.gs.error = (int *)(c->sync_words + 2);
+    a.info = c->info_dev;
     T = TranArgs{};
-    T.h = h;
     T.c_rp = t->c_rp; T.c_col = t->c_col; T.c_val = t->c_val;
     T.src_of_row = t->src_of_row; T.srow_ptr = t->srow_ptr; T.srow_src = t->srow_src; T.srow_sign = t->srow_sign;
     T.src = t->src; T.pwl = t->pwl; T.probe = t->probe; T.n_probes = t->n_probes; T.wave = t->wave;
     T.beff = t->beff; T.st = t->st;
-    fn = pick_tran(tran_lpr(t->n, nnz));
+    return OHM_OK;
+}
+
+// Cooperative grid of a transient kernel: up to two blocks per SM, no more
+// blocks than rows or devices need.
+static ohm_status tran_grid(ohm_transient *t, const void *fn, const KernelArgs &a, int &grid) {
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0));
     if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "transient kernel does not fit on an SM");
     per_sm = std::min(per_sm, 2);
     int64_t want = (t->n + kSolverBlock - 1) / kSolverBlock;
     want = std::max<int64_t>(want, ((int64_t)a.nd + a.nq + a.nm + kSolverBlock - 1) / kSolverBlock);
-    grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * c->num_sms));
-    a.gs.count = (unsigned long long *)c->sync_words;
-    a.gs.error = (int *)(c->sync_words + 2);
-    a.info = c->info_dev;
+    grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * t->ctx->num_sms));
     return OHM_OK;
+}
+
+// Kernel arguments of a fixed-step run on x_dev with step h: the companion
+// base A = G + C/h is formed (and copied to the assembled arrays), the run
+// record zeroed.  Returns the kernel and grid to launch.
+static ohm_status tran_prepare(ohm_transient *t, double *x_dev, double h, const ohm_newton_params *np,
+                               KernelArgs &a, TranArgs &T, TranFn &fn, int &grid, const double *&G) {
+    ohm_ctx *c = t->ctx;
+    ohm_status st = tran_args(t, x_dev, np, a, T, G);
+    if (st != OHM_OK) return st;
+    const int64_t nnz = t->nnz;
+    for (int phase = 0; phase < 3; ++phase) {
+        companion_kernel<<<steps_grid(phase == 1 ? t->c_nnz : nnz), 256, 0, c->stream>>>(
+            G, t->aval, a.vals64, a.vals32, nnz, t->c_slot, t->c_val, t->c_nnz, 1.0 / h, phase);
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaMemsetAsync(t->st, 0, sizeof(TranDev), c->stream));
+    T.h = h;
+    fn = pick_tran(tran_lpr(t->n, nnz));
+    return tran_grid(t, (const void *)fn, a, grid);
 }
 
 // One cooperative launch of steps [s0, s1).
@@ -484,6 +724,138 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
         info->fp64_fallbacks = d.fallbacks;
         info->launches = n_launch;
         info->graph = graph_used;
+        info->max_residual = d.max_residual;
+    }
+    return rs;
+}
+
+// Output arrays of a run: `points` rows of n_probes doubles (and times).
+static ohm_status ensure_wave(ohm_transient *t, int64_t points, bool times) {
+    const int64_t need = points * t->n_probes;
+    if (need > t->wave_cap) {
+        ohm_pool_free(t->wave);
+        t->wave = nullptr;
+        t->wave_cap = 0;
+        CUDA_TRY(dalloc(&t->wave, (size_t)need));
+        t->wave_cap = need;
+    }
+    if (times && points > t->times_cap) {
+        ohm_pool_free(t->times);
+        t->times = nullptr;
+        t->times_cap = 0;
+        CUDA_TRY(dalloc(&t->times, (size_t)points));
+        t->times_cap = points;
+    }
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_transient_run_adaptive(ohm_transient *t, double *x_dev, double tstep, double tstop,
+                                                 double tstart, const ohm_newton_params *np, int32_t max_points,
+                                                 double *times_host, double *waveforms_host,
+                                                 ohm_adaptive_info *info) {
+    if (!t || !x_dev || !np) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (!(tstep > 0.0) || !(tstop >= 0.0) || !std::isfinite(tstop) || !std::isfinite(tstart) || max_points < 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "need tstep > 0, finite tstop >= 0 and tstart, max_points >= 0");
+    if (np->continuation) return ohm_fail(OHM_ERR_INVALID_ARG, "continuation is for DC solves, not transient steps");
+    if (np->krylov.precond == OHM_PRECOND_ISAI1)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi");
+    ohm_ctx *c = t->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (np->initial_guess)
+        CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (!t->ad_st) {
+        cudaError_t e = t->put(&t->ad_xs, (const double *)nullptr, t->n);
+        if (e == cudaSuccess) e = t->put(&t->ad_xt, (const double *)nullptr, t->n);
+        if (e == cudaSuccess) e = t->put(&t->ad_fdev, (const double *)nullptr, t->n);
+        if (e == cudaSuccess) e = t->put(&t->ad_zeros, (const double *)nullptr, t->n);
+        if (e == cudaSuccess && t->n) e = cudaMemsetAsync(t->ad_zeros, 0, t->n * sizeof(double), c->stream);
+        if (e == cudaSuccess) e = t->put(&t->ad_st, (const AdaptDev *)nullptr, 1);
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "adaptive transient buffers: %s", cudaGetErrorString(e));
+    }
+    ohm_status st = ensure_wave(t, std::max<int64_t>(1, max_points), true);
+    if (st != OHM_OK) return st;
+    KernelArgs a;
+    TranArgs T;
+    const double *G = nullptr;
+    st = tran_args(t, x_dev, np, a, T, G);
+    if (st != OHM_OK) return st;
+    AdaptArgs P{};
+    P.tstep = tstep;
+    P.tstop = tstop;
+    P.tstart = tstart;
+    P.max_points = max_points;
+    P.nnz = t->nnz;
+    P.g_vals = G;
+    P.cg = t->cg;
+    P.zeros = t->ad_zeros;
+    P.aval = t->aval;
+    P.xs = t->ad_xs;
+    P.xt = t->ad_xt;
+    P.fdev = t->ad_fdev;
+    P.times = t->times;
+    P.st = t->ad_st;
+    const AdaptFn fn = pick_adaptive(tran_lpr(t->n, t->nnz));
+    int grid = 0;
+    st = tran_grid(t, (const void *)fn, a, grid);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaMemsetAsync(t->ad_st, 0, sizeof(AdaptDev), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->sync_words, 0, 4 * sizeof(unsigned int), c->stream));
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kSolverBlock);
+        cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, a, T, P));
+    }
+    // restore the plan's assembled system to its conductance base
+    restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
+    CUDA_TRY(cudaGetLastError());
+    AdaptDev d{};
+    unsigned int words[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(&d, t->ad_st, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int64_t kept = std::min<int64_t>(d.points, max_points);
+    if (kept > 0) {
+        if (times_host)
+            CUDA_TRY(cudaMemcpyAsync(times_host, t->times, kept * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (waveforms_host && t->n_probes)
+            CUDA_TRY(cudaMemcpyAsync(waveforms_host, t->wave, kept * t->n_probes * sizeof(double),
+                                     cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+    ohm_status rs = OHM_OK;
+    if (words[2] != 0) {
+        rs = ohm_fail(OHM_ERR_TIMEOUT, "a device barrier wait gave up (error word %u)", words[2]);
+    } else if (d.status == kAdTimestep) {
+        rs = ohm_fail(OHM_ERR_TIMESTEP, "simulation failed: %d consecutive failures at minimum timestep "
+                      "h_min=%.2e near t=%.2e", 10, tstep / 10000.0, d.t_fail);
+    } else if (d.status != 0) {
+        rs = ohm_fail(d.status == kErrSolve ? OHM_ERR_SOLVE
+                      : (d.status == kErrNewtonNumerical ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
+                      "%s solve of the step to t = %.6e failed (status %d, krylov code %d)",
+                      d.failed_kind == 1 ? "TRAP" : "BE", d.t_fail, d.status, d.kcode);
+    }
+    if (info) {
+        std::memset(info, 0, sizeof *info);
+        info->status = rs;
+        info->accepted = d.accepted;
+        info->rejected = d.rejected;
+        info->points = d.points;
+        info->newton_iterations = d.newton_its;
+        info->krylov_iterations = d.krylov_its;
+        info->linear_solves = d.solves;
+        info->fp64_fallbacks = d.fallbacks;
+        info->krylov_code = d.kcode;
+        info->failed_solve = d.status != 0 && d.status != kAdTimestep ? d.failed_kind : 0;
+        info->t_end = d.t;
+        info->h_last = d.h;
+        info->t_failed = d.t_fail;
         info->max_residual = d.max_residual;
     }
     return rs;

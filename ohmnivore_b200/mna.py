@@ -410,6 +410,61 @@ def compile_circuit(ckt: ck.Circuit) -> MnaSystem:
                      mosfet_components=mi, sources=sources)
 
 
+def uic_system(ckt: ck.Circuit, sysm: MnaSystem):
+    """The system of ``compute_uic_initial_conditions``
+    (``src/analysis/transient.rs:364-482``): G and b_dc with every inductor
+    branch row replaced by I_L = 0 and, per capacitor in component order,
+    the first unconstrained terminal row replaced by V(i) - V(j) = 0
+    (V(i) = 0 for a capacitor to ground); a node row is replaced once.
+    Returns (values on G's pattern, rhs); its solution is the UIC start."""
+    g = sysm.g
+    vals = g.val.astype(np.float64).copy()
+    b = sysm.b_dc.astype(np.float64).copy()
+    rp = g.row_ptr
+
+    def replace_row(r, entries):
+        vals[int(rp[r]):int(rp[r + 1])] = 0.0
+        for c, v in entries:
+            k = g.value_index(r, c)
+            if k is not None:
+                vals[k] = v
+        b[r] = 0.0
+
+    branch_row = np.full(ckt.n_components, -1, np.int64)
+    branch_row[sysm.branch_components] = sysm.n_nodes + np.arange(len(sysm.branch_components))
+    for ci in np.flatnonzero(ckt.kind == ck.L):
+        bk = int(branch_row[ci])
+        replace_row(bk, [(bk, 1.0)])
+    order = np.argsort(sysm.node_labels)
+    sorted_labels = sysm.node_labels[order]
+
+    def idx(label):
+        if label == 0:
+            return None
+        k = int(np.searchsorted(sorted_labels, label))
+        return int(order[k])
+
+    constrained = np.zeros(sysm.n_nodes, dtype=bool)
+    for ci in np.flatnonzero(ckt.kind == ck.C):
+        i, j = idx(int(ckt.nodes[ci, 0])), idx(int(ckt.nodes[ci, 1]))
+        if i is not None and j is None:
+            if not constrained[i]:
+                replace_row(i, [(i, 1.0)])
+                constrained[i] = True
+        elif i is None and j is not None:
+            if not constrained[j]:
+                replace_row(j, [(j, 1.0)])
+                constrained[j] = True
+        elif i is not None and j is not None:
+            if not constrained[i]:
+                replace_row(i, [(i, 1.0), (j, -1.0)])
+                constrained[i] = True
+            elif not constrained[j]:
+                replace_row(j, [(j, 1.0), (i, -1.0)])
+                constrained[j] = True
+    return vals, b
+
+
 def _ac_to_complex(mag, phase_deg):
     """``ac_to_complex`` (``src/compiler.rs:182-185``)."""
     ph = np.radians(phase_deg)

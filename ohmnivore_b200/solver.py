@@ -15,7 +15,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _lib
+from . import _lib, mna
 from ._lib import dptr, u32ptr, vptr
 
 DEFAULT_MAX_ITERATIONS = 10_000   # bicgstab.rs:10
@@ -58,6 +58,10 @@ class InvalidArgument(OhmnivoreError, ValueError):
     pass
 
 
+class TimestepError(OhmnivoreError):
+    """``OhmnivoreError::Timestep``: the adaptive step control gave up."""
+
+
 def _raise(st, info=None, x=None):
     msg = _lib.last_error()
     if st == _lib.ERR_SOLVE:
@@ -73,6 +77,8 @@ def _raise(st, info=None, x=None):
         raise DeviceTimeout(msg)
     if st == _lib.ERR_INVALID_ARG:
         raise InvalidArgument(msg)
+    if st == _lib.ERR_TIMESTEP:
+        raise TimestepError(msg)
     raise OhmnivoreError(f"status {st}: {msg}")
 
 
@@ -556,6 +562,15 @@ def adjoint_dc(plan: "NewtonPlan", x_dev_ptr: int, w, comps: ComponentTable, par
     return {"R": gr, "Is": gd}, lam, info.as_dict()
 
 
+def uic_initial_conditions(ckt, sysm, params: BiCgStabParams | None = None, ctx: Context | None = None):
+    """x(0) of a transient with UIC: the solution of ``mna.uic_system`` by
+    the GPU BiCGSTAB (compute_uic_initial_conditions,
+    src/analysis/transient.rs:364-482)."""
+    vals, b = mna.uic_system(ckt, sysm)
+    a = mna.Csr(sysm.size, sysm.size, sysm.g.row_ptr, sysm.g.col, vals)
+    return GpuSolver(ctx or default_context(), params or BiCgStabParams(tolerance=1e-14)).solve_real(a, b)
+
+
 def pack_sources(sysm):
     """``ohm_source`` records and PWL points for the sources of an MnaSystem
     (``collect_source_info``, src/analysis/transient.rs:212-262): a source
@@ -662,6 +677,33 @@ class Transient:
         if st != _lib.OK and check:
             _raise(st)
         return wave
+
+    def run_adaptive(self, x_dev_ptr: int, tstep: float, tstop: float, tstart: float = 0.0,
+                     params: NewtonParams | None = None, max_points: int | None = None, check: bool = True):
+        """The reference's adaptive BE / TRAP transient (transient::run,
+        src/analysis/transient.rs:77-178) from t = 0 to tstop on the device:
+        x (device pointer) holds x(0) and receives the last accepted state.
+        Returns (times, waveforms n_points x n_probes).  ``max_points``
+        defaults to 8 tstop / tstep + 2; a run that produced more points
+        returns the first max_points and reports the total in
+        ``last_info["points"]``."""
+        if max_points is None:
+            ok = tstep > 0 and np.isfinite(tstop) and tstop >= 0
+            max_points = int(8 * np.ceil(tstop / tstep)) + 2 if ok else 2   # bad values: the C call rejects them
+        p, keep = (params or NewtonParams()).to_c()
+        times = np.zeros(int(max_points))
+        wave = np.zeros((int(max_points), len(self.probes)))
+        info = _lib.AdaptiveInfo()
+        st = self.ctx.lib.ohm_transient_run_adaptive(self._h, C.c_void_p(int(x_dev_ptr)), float(tstep), float(tstop),
+                                                     float(tstart), C.byref(p), int(max_points),
+                                                     dptr(times) if times.size else None,
+                                                     dptr(wave) if wave.size else None, C.byref(info))
+        del keep
+        self.last_info = info.as_dict()
+        if st != _lib.OK and check:
+            _raise(st)
+        kept = min(info.points, int(max_points))
+        return times[:kept], wave[:kept]
 
 
 class DeviceBuffer:

@@ -10,6 +10,9 @@ only as the checker / timed CPU baseline.
   ``companion``     A = G + C/h (BE), transient.rs:285-323
   ``be_transient``  b = b(t_n) + (C/h) x_{n-1} (transient.rs:326-333), then the
                     Newton loop of ``newton_ref.newton`` on (A, b) from x_{n-1}.
+  ``adaptive_transient``  the adaptive BE / TRAP loop of transient::run
+                    (transient.rs:77-178): TRAP rhs :336-352, LTE :355-362.
+  ``uic_initial_conditions``  compute_uic_initial_conditions, transient.rs:364-482.
 
 The reference's transient is linear only (one linear solve per step, devices
 ignored); the Newton step per BE step is the nonlinear extension, so parity of
@@ -85,8 +88,10 @@ def b_at_time(sysm, t):
     return b
 
 
-def companion(sysm, h):
-    """A = G + C/h on G's pattern (every C entry must lie on it)."""
+def companion(sysm, h, alpha=1.0):
+    """A = G + (alpha / h) C on G's pattern (every C entry must lie on it),
+    form_companion_matrix, transient.rs:285-323."""
+    factor = alpha / h
     a = sysm.g.val.astype(np.float64).copy()
     c = sysm.c
     for i in range(c.nrows):
@@ -94,7 +99,7 @@ def companion(sysm, h):
             j = int(c.col[k])
             s = int(sysm.g.row_ptr[i]) + int(np.searchsorted(sysm.g.col[sysm.g.row_ptr[i]:sysm.g.row_ptr[i + 1]], j))
             assert sysm.g.col[s] == j, "capacitance entry off the conductance pattern"
-            a[s] += c.val[k] / h
+            a[s] += factor * c.val[k]
     return a
 
 
@@ -114,8 +119,136 @@ def be_transient(sysm, x0, t0, h, n_steps, probes, **newton_kw):
     its = []
     for s in range(n_steps):
         tn = t0 + (s + 1) * h
-        b = b_at_time(sysm, tn) + c_times(sysm, x) / h
+        b = b_at_time(sysm, tn) + (1.0 / h) * c_times(sysm, x)
         x, it = newton_ref.newton(sysm, base_vals=A, base_b=b, x0=x, **newton_kw)
         wave[s] = x[list(probes)]
         its.append(it)
     return x, wave, its
+
+
+class TimestepError(RuntimeError):
+    """``OhmnivoreError::Timestep`` (src/error.rs)."""
+
+
+def f_of_x(sysm, x):
+    """f(x) = G x + i(x): J(x) x - b of the system stamped at x on the base
+    (G, 0).  For a linear circuit this is the reference's G x."""
+    return -newton_ref.residual(sysm, x, base_vals=sysm.g.val, base_b=np.zeros(sysm.size))
+
+
+def adaptive_transient(sysm, x0, tstep, tstop, tstart, probes, **newton_kw):
+    """transient::run's stepping loop (transient.rs:77-178) from t = 0, each
+    companion solve a Newton solve (LU) from x_{n-1}.  Returns
+    (times, waveforms n_points x n_probes, stats)."""
+    h_min = tstep / 10_000.0
+    h_max = tstep
+    lte_tol = 1e-3
+    max_consecutive_failures = 10
+    probes = list(probes)
+    x = np.array(x0, dtype=np.float64)
+    times, wave = [], []
+    stats = {"accepted": 0, "rejected": 0, "linear_solves": 0}
+    if tstart <= 0.0:
+        times.append(0.0)
+        wave.append(x[probes].copy())
+    t = 0.0
+    h = min(tstep, h_max)
+    b_prev = b_at_time(sysm, 0.0)
+    use_be = True
+    fails = 0
+
+    def solve(alpha, rhs):
+        xs, _ = newton_ref.newton(sysm, base_vals=companion(sysm, h, alpha), base_b=rhs, x0=x, **newton_kw)
+        stats["linear_solves"] += 1
+        return xs
+
+    while t < tstop:
+        if t + h > tstop:
+            h = tstop - t
+        if h < h_min * 0.5:
+            break
+        t_next = t + h
+        b_next = b_at_time(sysm, t_next)
+        cx = c_times(sysm, x)
+        if use_be:
+            x_be = solve(1.0, b_next + (1.0 / h) * cx)
+            x_trap = x_be
+        else:
+            rhs = ((b_next + (2.0 / h) * cx) - f_of_x(sysm, x)) + b_prev
+            x_trap = solve(2.0, rhs)
+            x_be = solve(1.0, b_next + (1.0 / h) * cx)
+        if not use_be:
+            lte = (2.0 / 3.0) * float(np.max(np.abs(x_trap - x_be)))
+            ratio = lte_tol / lte if lte > 0.0 else math.inf
+            factor = min(max(0.9 * math.sqrt(ratio), 0.5), 2.0)
+            if lte > lte_tol:
+                h = max(h * factor, h_min)
+                fails += 1
+                if fails >= max_consecutive_failures and h <= h_min * 1.01:
+                    raise TimestepError(f"{fails} consecutive failures at minimum timestep near t={t:.2e}")
+                stats["rejected"] += 1
+                use_be = True
+                continue
+            h = min(max(h * factor, h_min), h_max)
+        else:
+            use_be = False
+        fails = 0
+        stats["accepted"] += 1
+        x = x_trap
+        b_prev = b_next
+        t = t_next
+        if t >= tstart:
+            times.append(t)
+            wave.append(x[probes].copy())
+    return np.array(times), np.array(wave).reshape(len(times), len(probes)), stats
+
+
+def uic_initial_conditions(sysm, ckt):
+    """compute_uic_initial_conditions (transient.rs:364-482): inductor branch
+    rows become I_L = 0; per capacitor, in component order, the first
+    unconstrained terminal row becomes V(i) - V(j) = 0 (V(i) = 0 to ground);
+    then one direct solve."""
+    from ohmnivore_b200 import circuits as ck
+
+    g = sysm.g
+    vals = g.val.astype(np.float64).copy()
+    b = sysm.b_dc.astype(np.float64).copy()
+    n_nodes = sysm.n_nodes
+
+    def zero_row(r):
+        vals[int(g.row_ptr[r]):int(g.row_ptr[r + 1])] = 0.0
+
+    def put(r, c, v):
+        k = g.value_index(r, c)
+        if k is not None:
+            vals[k] = v
+
+    branch_row = {int(ci): n_nodes + k for k, ci in enumerate(sysm.branch_components)}
+    for ci in range(ckt.n_components):
+        if ckt.kind[ci] == ck.L:
+            bk = branch_row[ci]
+            zero_row(bk)
+            put(bk, bk, 1.0)
+            b[bk] = 0.0
+    constrained = [False] * n_nodes
+
+    def idx(label):
+        return None if label == 0 else sysm.node_index(int(label))
+
+    for ci in range(ckt.n_components):
+        if ckt.kind[ci] != ck.C:
+            continue
+        i, j = idx(ckt.nodes[ci, 0]), idx(ckt.nodes[ci, 1])
+        if i is not None and j is None:
+            if not constrained[i]:
+                zero_row(i); put(i, i, 1.0); b[i] = 0.0; constrained[i] = True
+        elif i is None and j is not None:
+            if not constrained[j]:
+                zero_row(j); put(j, j, 1.0); b[j] = 0.0; constrained[j] = True
+        elif i is not None and j is not None:
+            if not constrained[i]:
+                zero_row(i); put(i, i, 1.0); put(i, j, -1.0); b[i] = 0.0; constrained[i] = True
+            elif not constrained[j]:
+                zero_row(j); put(j, j, 1.0); put(j, i, -1.0); b[j] = 0.0; constrained[j] = True
+    from .linear_ref import sparse_lu_solve
+    return sparse_lu_solve(sysm.size, g.row_ptr, g.col, vals, b)

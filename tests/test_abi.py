@@ -31,16 +31,17 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts(tmp_path):
     """ctypes mirrors agree with the C compiler's view of include/ohm.h."""
     src = tmp_path / "sz.c"
-    src.write_text('#include <stdio.h>\n#include "ohm.h"\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu",'
+    src.write_text('#include <stdio.h>\n#include "ohm.h"\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu",'
                    ' sizeof(ohm_krylov_params), sizeof(ohm_newton_params), sizeof(ohm_solve_info),'
                    ' sizeof(ohm_diode_desc), sizeof(ohm_bjt_desc), sizeof(ohm_mosfet_desc),'
-                   ' sizeof(ohm_source), sizeof(ohm_transient_info)); return 0;}\n')
+                   ' sizeof(ohm_source), sizeof(ohm_transient_info), sizeof(ohm_adaptive_info)); return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert sizes == [ctypes.sizeof(_lib.KrylovParams), ctypes.sizeof(_lib.NewtonParamsC),
                      ctypes.sizeof(_lib.SolveInfo), 48, 96, 64, _lib.SOURCE_DTYPE.itemsize,
-                     ctypes.sizeof(_lib.TransientInfo)]
+                     ctypes.sizeof(_lib.TransientInfo), ctypes.sizeof(_lib.AdaptiveInfo)]
+    assert ctypes.sizeof(_lib.AdaptiveInfo) == 80
     assert mna.DIODE_DTYPE.itemsize == 48
     assert mna.BJT_DTYPE.itemsize == 96
     assert mna.MOSFET_DTYPE.itemsize == 64
