@@ -53,8 +53,10 @@ def parse():
     p.add_argument("--tran-steps", type=int, default=2000)
     p.add_argument("--adjoint-rows", type=int, default=1000,
                    help="RC-diode mesh size of the adjoint measurement (0 skips it)")
-    p.add_argument("--sections", default="dc,batch,transient,adjoint",
-                   help="comma list of dc (the headline), batch, transient, adjoint; a run without dc "
+    p.add_argument("--grid-rows", type=int, default=1000,
+                   help="mesh size of the large-grid DC measurement (0 skips it)")
+    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid",
+                   help="comma list of dc (the headline), batch, transient, adjoint, grid; a run without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
@@ -238,6 +240,8 @@ def main():
             line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if "adjoint" in sections and args.adjoint_rows > 0:
             line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "grid" in sections and args.grid_rows > 0:
+            line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         plan.close()
@@ -390,6 +394,8 @@ def main():
         line["transient"] = transient_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if "adjoint" in sections and args.adjoint_rows > 0:
         line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+    if "grid" in sections and args.grid_rows > 0:
+        line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -561,6 +567,26 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
            "fp64": {"value": world * nsteps / (ms_d * 1e-3), "ms_full_run": ms_d,
                     "newton_iterations": info_d["newton_iterations"]},
            "mixed_vs_fp64_max_abs_diff_V": float(np.max(np.abs(wave_m - wave_d)))}
+    # the reference's own stepping policy on the same chain: adaptive BE / TRAP
+    # with LTE control (tstep 5 ps, one 2 ns input period), one launch
+    tstop_ad = 2e-9
+    with torch.cuda.stream(stream):
+        x.copy_(xdc)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    times_ad, _ = tr.run_adaptive(x.data_ptr(), h, tstop_ad, 0.0, step_params(True))
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    e1.synchronize()
+    ia = dict(tr.last_info)
+    ms_a = e0.elapsed_time(e1)
+    res["adaptive"] = {"workload": f"same chain, adaptive BE/TRAP, tstep 5 ps, tstop {tstop_ad * 1e9:g} ns",
+                       "ms_full_run": ms_a, "accepted": ia["accepted"], "rejected": ia["rejected"],
+                       "linear_solves": ia["linear_solves"], "newton_iterations": ia["newton_iterations"],
+                       "krylov_iterations": ia["krylov_iterations"], "points": ia["points"],
+                       "accepted_steps_per_s": ia["accepted"] / (ms_a * 1e-3),
+                       "min_step_ps": float(np.min(np.diff(times_ad))) * 1e12 if len(times_ad) > 1 else None}
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import newton_ref, transient_ref
         xd = xdc.cpu().numpy()
@@ -577,6 +603,59 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
         res["cpu_baseline"] = {"value": k / cpu_s, "unit": "timesteps/s", "cores": 1, "kind": "port",
                                "sample": f"{k} BE steps of the same chain, LU Newton per step, single thread"}
     tr.close()
+    plan.close()
+    return res
+
+
+def grid_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """DC operating point of the 1000x1000 RC mesh with diodes at 5 % of the
+    nodes (seed 4; the adjoint workload's circuit, capacitors open at DC,
+    the source at its step's final value, 1 V through 50 ohm):
+    one FP64 and one mixed-precision solve after a warm-up, with the
+    headline's Newton settings.  One large circuit fills the GPU, so the
+    batched kernel (one block per circuit) does not apply; the mixed path
+    is compared with the FP64 one."""
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    rows = args.grid_rows
+    ckt = circuits.rc_diode_mesh(rows, rows, seed=4)
+    src = int(np.flatnonzero(ckt.kind == circuits.V)[0])
+    ckt.value[src] = 1.0                           # DC at the step's final value
+    ckt.tran.pop(src, None)
+    sysm = mna.compile_circuit(ckt)
+    plan = S.NewtonPlan(sysm, ctx)
+    x = torch.zeros(sysm.size, dtype=torch.float64, device=f"cuda:{local_rank}")
+
+    def solve(mixed):
+        with torch.cuda.stream(stream):
+            x.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        info = plan.newton_device(x.data_ptr(), newton_params(mixed))
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=x.device)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), info, x.cpu().numpy()
+
+    solve(False)                                   # warm-up
+    ms_d, info_d, x_d = solve(False)
+    ms_m, info_m, x_m = solve(True)
+    nn = sysm.n_nodes
+    res = {"workload": f"DC operating point, {rows}x{rows} RC-diode mesh, 1 V through 50 ohm ({sysm.size} rows, "
+                       f"{sysm.g.nnz} nonzeros, {len(sysm.diode_descriptors)} diodes)",
+           "fp64": {"value": world * 1e3 / ms_d, "unit": "solves/s", "ms": ms_d,
+                    "newton_iterations": info_d["iterations"], "krylov_iterations": info_d["krylov_iterations"]},
+           "mixed": {"value": world * 1e3 / ms_m, "unit": "solves/s", "ms": ms_m,
+                     "newton_iterations": info_m["iterations"], "krylov_iterations": info_m["krylov_iterations"],
+                     "fp64_fallbacks": info_m["fp64_fallbacks"]},
+           "mixed_vs_fp64": ms_d / ms_m,
+           "mixed_vs_fp64_rel_err_voltages": float(np.max(np.abs(x_m[:nn] - x_d[:nn])) / np.max(np.abs(x_d[:nn])))}
     plan.close()
     return res
 
