@@ -487,6 +487,40 @@ ohm_status ohm_batch_autotune(ohm_batch *batch, const ohm_newton_params *params,
 ohm_status ohm_batch_set_kernel(ohm_batch *batch, int32_t lanes_per_row, int32_t threads_per_block,
                                 int32_t blocks_per_sm);
 
+/* ---------------------------------------------------------------- compile --
+ * Device-side MNA compile of compile (src/compiler.rs:194-754): node
+ * numbering by first appearance, branch rows for V sources and inductors,
+ * the stamps as CSR triplets summed in triplet order (CsrMatrix::from_triplets,
+ * src/sparse.rs:51-104), GMIN and C's pattern zero-filled into G, the DC
+ * right-hand side and the device descriptors (slots by value_index), all on
+ * the GPU.  The result equals the reference's compile output bit for bit.
+ *
+ * Components in column form: kind[m] (0 R, 1 C, 2 L, 3 V, 4 I, 5 D, 6 Q,
+ * 7 M, the order of the reference's Component enum); nodes[m x 3] labels,
+ * <= 0 meaning ground, the third used only by BJTs (emitter) and MOSFETs
+ * (source); value[m] (R ohms, C farads, L henries, V/I DC value, NaN = no
+ * DC value); params[m x 7] (D: is, n; Q: is, bf, br, nf, nr, npn != 0;
+ * M: vto, kp, lambda, nmos != 0).  OHM_ERR_COMPILE names the first
+ * zero resistance, negative capacitance or device without a model
+ * (compiler.rs:310-316, 336-340), in that order of checks. */
+typedef struct {
+    int64_t n_nodes, size, n_branches, g_nnz, c_nnz, n_diodes, n_bjts, n_mosfets;
+} ohm_netlist_sizes;
+
+typedef struct ohm_netlist ohm_netlist;
+ohm_status ohm_compile(ohm_ctx *ctx, int64_t m, const int32_t *kind, const int64_t *nodes, const double *value,
+                       const double *params, ohm_netlist **out);
+ohm_status ohm_netlist_get_sizes(const ohm_netlist *netlist, ohm_netlist_sizes *out);
+/* Copies the compiled system to host arrays (any may be NULL): G and C in
+ * CSR (size + 1 row pointers, nnz columns and values), b_dc (size), the
+ * node labels in matrix order (n_nodes), the component index of each branch
+ * row (n_branches) and the descriptors. */
+ohm_status ohm_netlist_download(const ohm_netlist *netlist, uint32_t *g_row_ptr, uint32_t *g_col, double *g_val,
+                                uint32_t *c_row_ptr, uint32_t *c_col, double *c_val, double *b_dc,
+                                int64_t *node_labels, int64_t *branch_components, ohm_diode_desc *diodes,
+                                ohm_bjt_desc *bjts, ohm_mosfet_desc *mosfets);
+ohm_status ohm_netlist_destroy(ohm_netlist *netlist);
+
 #ifdef __cplusplus
 }
 #endif

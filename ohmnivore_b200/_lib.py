@@ -69,6 +69,11 @@ class AdaptiveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class NetlistSizes(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("n_nodes", "size", "n_branches", "g_nnz", "c_nnz", "n_diodes",
+                                          "n_bjts", "n_mosfets")]
+
+
 # ohm_source (include/ohm.h), 104 bytes
 SOURCE_DTYPE = np.dtype([("kind", "<i4"), ("n_rows", "<i4"), ("rows", "<u4", (2,)), ("sign", "<f8", (2,)),
                          ("dc", "<f8"), ("p", "<f8", (7,)), ("pwl_offset", "<i4"), ("pwl_count", "<i4")],
@@ -154,6 +159,12 @@ SIGNATURES = {
                                _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                     C.POINTER(NewtonParamsC), C.c_int32, _dp, C.POINTER(TransientInfo)]),
+    "ohm_compile": (C.c_int, [_vp, _i64, C.POINTER(C.c_int32), C.POINTER(C.c_int64), _dp, _dp,
+                              C.POINTER(C.c_void_p)]),
+    "ohm_netlist_get_sizes": (C.c_int, [_vp, C.POINTER(NetlistSizes)]),
+    "ohm_netlist_download": (C.c_int, [_vp, _u32p, _u32p, _dp, _u32p, _u32p, _dp, _dp, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64), _vp, _vp, _vp]),
+    "ohm_netlist_destroy": (C.c_int, [_vp]),
     "ohm_transient_run_adaptive": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double,
                                              C.POINTER(NewtonParamsC), C.c_int32, _dp, _dp,
                                              C.POINTER(AdaptiveInfo)]),

@@ -312,15 +312,10 @@ def compile_circuit(ckt: ck.Circuit) -> MnaSystem:
 
     # RHS (compiler.rs:391-398 V sources, 440-468 I sources).
     b_dc = np.zeros(size)
-    b_ac = np.zeros(size, dtype=np.complex128)
     vmask = kind == ck.V
     vdc = vmask & ~np.isnan(ckt.value)
     b_dc[bk[vdc]] = ckt.value[vdc]
-    vac = vmask & ~np.isnan(ckt.ac[:, 0])
-    if vac.any():
-        b_ac[bk[vac]] = _ac_to_complex(ckt.ac[vac, 0], ckt.ac[vac, 1])
     imask = kind == ck.I
-    sources = []
     idc = np.flatnonzero(imask & ~np.isnan(ckt.value))
     if idc.size:
         ii = ni[idc]
@@ -331,22 +326,7 @@ def compile_circuit(ckt: ck.Circuit) -> MnaSystem:
         amt = np.stack([-val, val], axis=1).ravel()
         ok = tgt >= 0
         np.add.at(b_dc, tgt[ok], amt[ok])
-    iac = np.flatnonzero(imask & ~np.isnan(ckt.ac[:, 0]))
-    if iac.size:
-        z = _ac_to_complex(ckt.ac[iac, 0], ckt.ac[iac, 1])
-        tgt = np.stack([ni[iac], nj[iac]], axis=1).ravel()
-        amt = np.stack([-z, z], axis=1).ravel()
-        ok = tgt >= 0
-        np.add.at(b_ac, tgt[ok], amt[ok])
-    # Time-dependent sources for the transient driver (transient.rs:232-262).
-    for ci in np.flatnonzero(vmask | imask):
-        ci = int(ci)
-        if kind[ci] == ck.V:
-            entries = [(int(bk[ci]), 1.0)]
-        else:
-            entries = [(int(x), s) for x, s in ((ni[ci], -1.0), (nj[ci], 1.0)) if x >= 0]
-        dcv = None if np.isnan(ckt.value[ci]) else float(ckt.value[ci])
-        sources.append((ci, entries, dcv, ckt.tran.get(ci)))
+    b_ac, sources = _ac_rhs_and_sources(ckt, ni, nj, bk, size)
 
     # V-source constrained nodes (compiler.rs:582-595).
     fixed = np.zeros(max(n_nodes, 1), dtype=bool)
@@ -408,6 +388,69 @@ def compile_circuit(ckt: ck.Circuit) -> MnaSystem:
                      diode_descriptors=dd, bjt_descriptors=qd, mosfet_descriptors=md,
                      bjt_vaf=vaf, diode_components=di, bjt_components=qi,
                      mosfet_components=mi, sources=sources)
+
+
+def _ac_rhs_and_sources(ckt: ck.Circuit, ni, nj, bk, size):
+    """AC right-hand side (compiler.rs:391-398, 440-468: V sources at their
+    branch rows, current sources -I / +I at their nodes in component order)
+    and the time-dependent sources of the transient driver
+    (transient.rs:232-262) as [(component, [(row, sign)], dc, tran)]."""
+    kind = ckt.kind
+    b_ac = np.zeros(size, dtype=np.complex128)
+    vmask = kind == ck.V
+    imask = kind == ck.I
+    vac = vmask & ~np.isnan(ckt.ac[:, 0])
+    if vac.any():
+        b_ac[bk[vac]] = _ac_to_complex(ckt.ac[vac, 0], ckt.ac[vac, 1])
+    iac = np.flatnonzero(imask & ~np.isnan(ckt.ac[:, 0]))
+    if iac.size:
+        z = _ac_to_complex(ckt.ac[iac, 0], ckt.ac[iac, 1])
+        tgt = np.stack([ni[iac], nj[iac]], axis=1).ravel()
+        amt = np.stack([-z, z], axis=1).ravel()
+        ok = tgt >= 0
+        np.add.at(b_ac, tgt[ok], amt[ok])
+    sources = []
+    for ci in np.flatnonzero(vmask | imask):
+        ci = int(ci)
+        if kind[ci] == ck.V:
+            entries = [(int(bk[ci]), 1.0)]
+        else:
+            entries = [(int(x), sg) for x, sg in ((ni[ci], -1.0), (nj[ci], 1.0)) if x >= 0]
+        dcv = None if np.isnan(ckt.value[ci]) else float(ckt.value[ci])
+        sources.append((ci, entries, dcv, ckt.tran.get(ci)))
+    return b_ac, sources
+
+
+def system_from_device_compile(ckt: ck.Circuit, g: Csr, c: Csr, b_dc, node_labels, branch_components,
+                               dd, qd, md) -> MnaSystem:
+    """An :class:`MnaSystem` from the arrays of the device compile: the AC
+    rhs, the source list and the per-kind index maps are filled in on the
+    host (small, per-source work)."""
+    n_nodes = int(node_labels.shape[0])
+    size = n_nodes + int(branch_components.shape[0])
+    order = np.argsort(node_labels, kind="stable")
+    sorted_labels = node_labels[order]
+
+    def nidx(lbl):
+        lbl = np.asarray(lbl, np.int64)
+        out = np.full(lbl.shape, -1, np.int64)
+        ok = lbl > 0
+        if ok.any() and n_nodes:
+            out[ok] = order[np.searchsorted(sorted_labels, lbl[ok])]
+        return out
+
+    ni, nj = nidx(ckt.nodes[:, 0]), nidx(ckt.nodes[:, 1])
+    bk = np.full(ckt.n_components, -1, np.int64)
+    bk[branch_components] = n_nodes + np.arange(branch_components.shape[0])
+    b_ac, sources = _ac_rhs_and_sources(ckt, ni, nj, bk, size)
+    qi = np.flatnonzero(ckt.kind == ck.Q)
+    vaf = ckt.params[qi, 6].copy()
+    vaf[np.isnan(vaf)] = np.inf
+    return MnaSystem(g=g, c=c, b_dc=b_dc, b_ac=b_ac, size=size, n_nodes=n_nodes,
+                     node_labels=node_labels, branch_components=branch_components,
+                     diode_descriptors=dd, bjt_descriptors=qd, mosfet_descriptors=md,
+                     bjt_vaf=vaf, diode_components=np.flatnonzero(ckt.kind == ck.D), bjt_components=qi,
+                     mosfet_components=np.flatnonzero(ckt.kind == ck.M), sources=sources)
 
 
 def uic_system(ckt: ck.Circuit, sysm: MnaSystem):

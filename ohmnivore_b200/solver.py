@@ -562,6 +562,55 @@ def adjoint_dc(plan: "NewtonPlan", x_dev_ptr: int, w, comps: ComponentTable, par
     return {"R": gr, "Is": gd}, lam, info.as_dict()
 
 
+def compile_circuit_device(ckt, ctx: Context | None = None) -> "mna.MnaSystem":
+    """``compile`` (src/compiler.rs:194-754) on the GPU (``ohm_compile``):
+    the same :class:`mna.MnaSystem` as ``mna.compile_circuit``, bit for bit.
+    Raises ``mna.CompileError`` for the reference's compile errors."""
+    ctx = ctx or default_context()
+    m = ckt.n_components
+    kind = np.ascontiguousarray(ckt.kind, dtype=np.int32)
+    nodes = np.ascontiguousarray(ckt.nodes, dtype=np.int64).reshape(m, 3)
+    value = np.ascontiguousarray(ckt.value, dtype=np.float64)
+    params = np.ascontiguousarray(ckt.params, dtype=np.float64).reshape(m, 7)
+    h = C.c_void_p()
+    st = ctx.lib.ohm_compile(ctx.handle, m, kind.ctypes.data_as(C.POINTER(C.c_int32)),
+                             nodes.ctypes.data_as(C.POINTER(C.c_int64)), dptr(value), dptr(params), C.byref(h))
+    if st == _lib.ERR_COMPILE:
+        raise mna.CompileError(_lib.last_error())
+    if st != _lib.OK:
+        _raise(st)
+    try:
+        z = _lib.NetlistSizes()
+        st = ctx.lib.ohm_netlist_get_sizes(h, C.byref(z))
+        if st != _lib.OK:
+            _raise(st)
+        n = int(z.size)
+        g_rp = np.zeros(n + 1, np.uint32)
+        g_col = np.zeros(z.g_nnz, np.uint32)
+        g_val = np.zeros(z.g_nnz)
+        c_rp = np.zeros(n + 1, np.uint32)
+        c_col = np.zeros(z.c_nnz, np.uint32)
+        c_val = np.zeros(z.c_nnz)
+        b_dc = np.zeros(n)
+        labels = np.zeros(z.n_nodes, np.int64)
+        branches = np.zeros(z.n_branches, np.int64)
+        dd = np.zeros(z.n_diodes, dtype=mna.DIODE_DTYPE)
+        qd = np.zeros(z.n_bjts, dtype=mna.BJT_DTYPE)
+        md = np.zeros(z.n_mosfets, dtype=mna.MOSFET_DTYPE)
+        i64 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))  # noqa: E731
+        st = ctx.lib.ohm_netlist_download(h, u32ptr(g_rp), u32ptr(g_col), dptr(g_val), u32ptr(c_rp), u32ptr(c_col),
+                                          dptr(c_val), dptr(b_dc), i64(labels), i64(branches),
+                                          C.c_void_p(dd.ctypes.data), C.c_void_p(qd.ctypes.data),
+                                          C.c_void_p(md.ctypes.data))
+        if st != _lib.OK:
+            _raise(st)
+    finally:
+        ctx.lib.ohm_netlist_destroy(h)
+    g = mna.Csr(n, n, g_rp.astype(np.int64), g_col.astype(np.int64), g_val)
+    c = mna.Csr(n, n, c_rp.astype(np.int64), c_col.astype(np.int64), c_val)
+    return mna.system_from_device_compile(ckt, g, c, b_dc, labels, branches, dd, qd, md)
+
+
 def uic_initial_conditions(ckt, sysm, params: BiCgStabParams | None = None, ctx: Context | None = None):
     """x(0) of a transient with UIC: the solution of ``mna.uic_system`` by
     the GPU BiCGSTAB (compute_uic_initial_conditions,
