@@ -55,8 +55,8 @@ def parse():
                    help="RC-diode mesh size of the adjoint measurement (0 skips it)")
     p.add_argument("--grid-rows", type=int, default=1000,
                    help="mesh size of the large-grid DC measurement (0 skips it)")
-    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid",
-                   help="comma list of dc (the headline), batch, transient, adjoint, grid; a run without dc "
+    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid,compile",
+                   help="comma list of dc (the headline), batch, transient, adjoint, grid, compile; a run without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
     p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
@@ -242,6 +242,8 @@ def main():
             line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if "grid" in sections and args.grid_rows > 0:
             line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "compile" in sections:
+            line["compile"] = compile_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         plan.close()
@@ -396,6 +398,8 @@ def main():
         line["adjoint"] = adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if "grid" in sections and args.grid_rows > 0:
         line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+    if "compile" in sections:
+        line["compile"] = compile_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -604,6 +608,46 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
                                "sample": f"{k} BE steps of the same chain, LU Newton per step, single thread"}
     tr.close()
     plan.close()
+    return res
+
+
+def compile_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """Device-side MNA compile (ohm_compile) against the host compiler on the
+    workloads' circuits: wall time of each (the device figure includes the
+    upload of the component arrays, the download of the system and its
+    assembly into the same Python object), and a bit-for-bit check."""
+    from ohmnivore_b200 import circuits, mna
+    work = [("diode mesh 500x500 (headline)", lambda: circuits.diode_mesh(500, 500, seed=1)),
+            ("RC-diode mesh 1000x1000", lambda: circuits.rc_diode_mesh(1000, 1000, seed=4)),
+            ("inverter chain, 100,000 stages", lambda: circuits.inverter_chain(stages=100_000, seed=2))]
+    S.compile_circuit_device(circuits.diode_mesh(8, 8, seed=1), ctx)        # module load, memory cache
+    res = {}
+    for name, mk in work:
+        ckt = mk()
+        t0 = time.perf_counter()
+        host = mna.compile_circuit(ckt)
+        t1 = time.perf_counter()
+        dev = S.compile_circuit_device(ckt, ctx)
+        t2 = time.perf_counter()
+        same = (np.array_equal(dev.g.col, host.g.col) and np.array_equal(dev.g.row_ptr, host.g.row_ptr)
+                and np.array_equal(dev.g.val.view(np.uint64), host.g.val.view(np.uint64))
+                and np.array_equal(dev.b_dc.view(np.uint64), host.b_dc.view(np.uint64))
+                and np.array_equal(dev.diode_descriptors.view(np.uint8), host.diode_descriptors.view(np.uint8))
+                and np.array_equal(dev.mosfet_descriptors.view(np.uint8), host.mosfet_descriptors.view(np.uint8)))
+        res[name] = {"rows": host.size, "nonzeros": host.g.nnz, "components": ckt.n_components,
+                     "host_s": t1 - t0, "device_s": t2 - t1, "speedup": (t1 - t0) / (t2 - t1),
+                     "bit_identical": bool(same)}
+    # many small circuits: 32 Monte Carlo instances, one call each
+    ckts = circuits.monte_carlo_batch(32, seed=3, vaf=100.0)
+    t0 = time.perf_counter()
+    hs = [mna.compile_circuit(c) for c in ckts]
+    t1 = time.perf_counter()
+    ds = [S.compile_circuit_device(c, ctx) for c in ckts]
+    t2 = time.perf_counter()
+    same = all(np.array_equal(d.g.val.view(np.uint64), h.g.val.view(np.uint64)) for d, h in zip(ds, hs))
+    res["32 Monte Carlo circuits, one call each"] = {
+        "rows": int(sum(h.size for h in hs)), "host_s": t1 - t0, "device_s": t2 - t1,
+        "speedup": (t1 - t0) / (t2 - t1), "bit_identical": bool(same)}
     return res
 
 
