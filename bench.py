@@ -59,8 +59,10 @@ def parse():
                    help="comma list of dc (the headline), batch, transient, adjoint, grid, compile; a run without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
-    p.add_argument("--profile", choices=["fp64", "mixed"], default=None,
-                   help="one warm-up and one timed solve only (for an ncu capture)")
+    p.add_argument("--profile", choices=["fp64", "mixed", "grid"], default=None,
+                   help="one warm-up and one timed solve only (for an ncu capture); 'grid': the "
+                        "--grid-rows RC-diode mesh at 1 V, one Newton iteration with BiCGSTAB capped at "
+                        "40 iterations (a launch of a few ms on a working set larger than L2)")
     return p.parse_args()
 
 
@@ -806,6 +808,29 @@ def run_profile_case(args):
     import torch
     from ohmnivore_b200 import circuits, mna
     from ohmnivore_b200 import solver as S
+    if args.profile == "grid":
+        ckt = circuits.rc_diode_mesh(args.grid_rows, args.grid_rows, seed=4)
+        src = int(np.flatnonzero(ckt.kind == circuits.V)[0])
+        ckt.value[src] = 1.0
+        ckt.tran.pop(src, None)
+        sysm = mna.compile_circuit(ckt)
+        ctx = S.Context(0)
+        plan = S.NewtonPlan(sysm, ctx)
+        x = torch.zeros(sysm.size, dtype=torch.float64, device="cuda")
+        params = S.NewtonParams(max_iterations=1, abs_tol=1e-9, bicgstab_max_iterations=40,
+                                bicgstab_tolerance=1e-14, inner_rtol=1e-12)
+        for _ in range(2):
+            x.zero_()
+            torch.cuda.synchronize()
+            try:
+                plan.newton_device(x.data_ptr(), params)
+            except (S.SolveError, S.NewtonNotConverged):
+                pass                     # the capped Krylov solve is expected to stop unconverged
+        print(json.dumps({"profile_case": f"RC-diode mesh {args.grid_rows}x{args.grid_rows} at 1 V, one Newton "
+                                          "iteration, 40 BiCGSTAB iterations", **plan.last_info}))
+        plan.close()
+        ctx.close()
+        return
     sysm = mna.compile_circuit(circuits.diode_mesh(args.rows, args.cols, seed=1))
     ctx = S.Context(0)
     plan = S.NewtonPlan(sysm, ctx)
