@@ -184,6 +184,84 @@ __device__ __forceinline__ void gather_max(const double *partials, double (&out)
     __syncthreads();
 }
 
+// Grid all-reduce (sum, or max when MAX) of NV <= 4 values in one grid
+// barrier and three block synchronisations: warps reduce to shared memory;
+// warp 0 forms the block value (the same fixed tree as block_sum /
+// block_max) and its lane 0 publishes it to partials[k * G + block],
+// arrives on the barrier counter (release) and waits for every block
+// (acquire, bounded); then warp k sums the G partials of value k in a fixed
+// order and every thread reads the results.  The arithmetic is that of
+// publish_partials + grid_barrier + gather_partials, so the results are
+// bit-identical to it; `smem` holds >= 32 * 4 + 4 doubles.  Returns false
+// when the barrier wait gave up.
+template <int NV, bool MAX>
+__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials, const GridSync &gs,
+                                               unsigned long long &epoch, double *smem) {
+    __shared__ int s_ok;
+    const int G = gridDim.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    double *res = smem + 32 * 4;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = MAX ? fmax(x, y) : x + y;
+        }
+        if (lane == 0) smem[k * 32 + warp] = x;
+    }
+    epoch += gridDim.x;
+    __syncthreads();
+    if (warp == 0) {
+        double b[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = (lane < nwarps) ? smem[k * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = MAX ? fmax(x, y) : x + y;
+            }
+            b[k] = x;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) partials[k * G + blockIdx.x] = b[k];
+            red_release_add_u64(gs.count, 1ull);
+            int ok = 1;
+            uint32_t spins = 0;
+            while (ld_acquire_u64(gs.count) < epoch) {
+                if (++spins > kBarrierSpinLimit) {
+                    atomicCAS(gs.error, 0, kStatusTimeout);
+                    ok = 0;
+                    break;
+                }
+                if (spins > kTightSpins) __nanosleep(64);
+            }
+            s_ok = ok;
+        }
+    }
+    __syncthreads();
+    if (!s_ok) return false;
+    if (warp < NV) {
+        const double *p = partials + (size_t)warp * G;
+        double x = 0.0;
+#pragma unroll 4
+        for (int j = lane; j < G; j += 32) x = MAX ? fmax(x, __ldcg(p + j)) : x + __ldcg(p + j);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = MAX ? fmax(x, y) : x + y;
+        }
+        if (lane == 0) res[warp] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = res[k];
+    return true;
+}
+
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
 }  // namespace ohm

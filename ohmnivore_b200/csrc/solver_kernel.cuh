@@ -211,19 +211,11 @@ struct GridTeam {
     }
     template <int NV>
     __device__ __forceinline__ bool allreduce(double (&v)[NV]) {
-        double *pr = part();
-        publish_partials<NV>(v, pr, smem);
-        if (!sync()) return false;
-        gather_partials<NV>(pr, v, smem);
-        return true;
+        return grid_allreduce<NV, false>(v, part(), gs, epoch, smem);
     }
     template <int NV>
     __device__ __forceinline__ bool allmax(double (&v)[NV]) {
-        double *pr = part();
-        publish_max<NV>(v, pr, smem);
-        if (!sync()) return false;
-        gather_max<NV>(pr, v, smem);
-        return true;
+        return grid_allreduce<NV, true>(v, part(), gs, epoch, smem);
     }
 };
 
@@ -1068,7 +1060,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
 // One large system per launch: the whole (co-resident) grid is the team.
 template <int LPR>
 __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
-    __shared__ double smem[32 * 4];
+    __shared__ double smem[32 * 4 + 4];   // GridTeam reductions: warp values + results
     GridTeam g;
     g.G = gridDim.x;
     g.bid = blockIdx.x;
