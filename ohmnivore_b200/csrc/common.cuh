@@ -214,7 +214,6 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials
     epoch += gridDim.x;
     __syncthreads();
     if (warp == 0) {
-        double b[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             double x = (lane < nwarps) ? smem[k * 32 + lane] : 0.0;
@@ -223,11 +222,9 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials
                 const double y = __shfl_xor_sync(0xffffffffu, x, o);
                 x = MAX ? fmax(x, y) : x + y;
             }
-            b[k] = x;
+            if (lane == 0) partials[k * G + blockIdx.x] = x;
         }
         if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) partials[k * G + blockIdx.x] = b[k];
             red_release_add_u64(gs.count, 1ull);
             int ok = 1;
             uint32_t spins = 0;
