@@ -254,7 +254,7 @@ struct Workspace {
     double *vec = nullptr;       // 15 * n doubles
     double *r64 = nullptr;
     double *dx = nullptr;
-    double *partials = nullptr;  // 64 per SM (>= 16 x the largest grid, 2 blocks per SM)
+    double *partials = nullptr;  // 8 * max grid
     int32_t *partner = nullptr;
     uint32_t *diag_slot = nullptr, *off_slot = nullptr;
     uint8_t *rowflag = nullptr;

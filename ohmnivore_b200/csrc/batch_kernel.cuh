@@ -28,7 +28,7 @@ __device__ __forceinline__ P *offset(P *p, int64_t k) { return p ? p + k : p; }
 
 template <int LPR, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_solver(BatchArgs B) {
-    __shared__ double smem[32 * 8];     // block reductions of up to 8 values
+    __shared__ double smem[32 * 4];
     __shared__ int s_q;
     for (;;) {
         if (threadIdx.x == 0) s_q = (int)atomicAdd(B.queue, 1u);

@@ -184,7 +184,7 @@ __device__ __forceinline__ void gather_max(const double *partials, double (&out)
     __syncthreads();
 }
 
-// Grid all-reduce (sum, or max when MAX) of NV <= 8 values in one grid
+// Grid all-reduce (sum, or max when MAX) of NV <= 4 values in one grid
 // barrier and three block synchronisations: warps reduce to shared memory;
 // warp 0 forms the block value (the same fixed tree as block_sum /
 // block_max) and its lane 0 publishes it to partials[k * G + block],
@@ -192,7 +192,7 @@ __device__ __forceinline__ void gather_max(const double *partials, double (&out)
 // (acquire, bounded); then warp k sums the G partials of value k in a fixed
 // order and every thread reads the results.  The arithmetic is that of
 // publish_partials + grid_barrier + gather_partials, so the results are
-// bit-identical to it; `smem` holds >= 32 * 8 + 8 doubles.  Returns false
+// bit-identical to it; `smem` holds >= 32 * 4 + 4 doubles.  Returns false
 // when the barrier wait gave up.
 template <int NV, bool MAX>
 __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials, const GridSync &gs,
@@ -200,7 +200,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials
     __shared__ int s_ok;
     const int G = gridDim.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = (blockDim.x + 31) >> 5;
-    double *res = smem + 32 * 8;
+    double *res = smem + 32 * 4;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
         double x = v[k];

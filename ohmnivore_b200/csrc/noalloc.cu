@@ -38,8 +38,8 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffVec = 0;                                               // 15 x rows x 8
 constexpr size_t kOffR64 = kOffVec + align256(15 * kMaxRows * 8);
 constexpr size_t kOffDx = kOffR64 + align256(kMaxRows * 8);
-constexpr size_t kOffPartials = kOffDx + align256(kMaxRows * 8);            // 16 x grid doubles
-constexpr size_t kOffPartner = kOffPartials + align256(16 * kMaxGrid * 8);
+constexpr size_t kOffPartials = kOffDx + align256(kMaxRows * 8);            // 8 x grid doubles
+constexpr size_t kOffPartner = kOffPartials + align256(8 * kMaxGrid * 8);
 constexpr size_t kOffDiag = kOffPartner + align256(kMaxRows * 4);
 constexpr size_t kOffOff = kOffDiag + align256(kMaxRows * 4);
 constexpr size_t kOffCand = kOffOff + align256(kMaxRows * 4);

@@ -176,7 +176,7 @@ struct KernelArgs {
     const uint32_t *mu_rp, *mu_col, *mu_cp, *mu_row, *mu_pos;
     double *mu_val;
 
-    double *partials;           // >= 16 * gridDim.x doubles (two alternating regions of 8 values)
+    double *partials;           // >= 8 * gridDim.x doubles (two alternating regions)
     GridSync gs;
     DeviceInfo *info;
 };
@@ -205,7 +205,7 @@ struct GridTeam {
     // block may publish reduction j+1 while a slower block still reads
     // reduction j, but never reduction j+2 (a barrier separates them).
     __device__ __forceinline__ double *part() {
-        double *p = partials + (size_t)(red & 1) * 8 * G;
+        double *p = partials + (size_t)(red & 1) * 4 * G;
         ++red;
         return p;
     }
@@ -341,20 +341,12 @@ struct KrylovOut {
 };
 
 // Right-preconditioned BiCGSTAB on J d = r64 in precision T, d0 = 0, with
-// the reference's operation order (bicgstab.rs:104-183) and two grid
+// the reference's operation order (bicgstab.rs:104-183) and three grid
 // synchronisations per iteration:
-//   AB: r = s - w t and p = (p - w v) b + r, both formed on the fly per
-//       gathered row (the row's record and its s, t), v = A M^-1 p with
-//       M^-1 p formed the same way; the owner also finishes the previous
-//       step d += a phat + w shat; reduce (r_hat, v), (v, v)
-//   CD: s = r - a v and t = A M^-1 s (on the fly); reduce (s, s), (t, s),
-//       (t, t), (r_hat, s), (r_hat, t) and their W-scaled forms
-// The reductions of the residual update r = s - w t then follow without a
-// third synchronisation: (r_hat, r) = (r_hat, s) - w (r_hat, t) and
-// ||r||^2 = ||s||^2 - 2 w (t, s) + w^2 ||t||^2 (same for W r).  Every vector
-// value is rounded as in the three-phase form; a convergence the recurrence
-// reports is confirmed by the true ||W r|| (one extra reduction on that
-// iteration only), since the recurrence can lose digits to cancellation.
+//   AB: p = (p - w v) b + r and v = A M^-1 p  (M^-1 p formed on the fly per
+//       gathered record), reduce (r_hat, v), (v, v)
+//   CD: s = r - a v and t = A M^-1 s (on the fly), reduce (s, s), (t, s), (t, t)
+//   E : d += a phat + w shat; r = s - w t, reduce (r_hat, r), (r, r)
 // The early exit on ||s|| (bicgstab.rs:134-139) is taken after CD; t is then
 // simply unused.  Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On
 // success the correction is left in a.dx (FP64) for the rows of this block.
@@ -408,8 +400,6 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
         KRec<T> q;
         q.p = T(0); q.v = T(0); q.r = rt; q.c = cvt<T>(cs);
         cur[i] = q;
-        s[i] = rt;                   // r = s - w t before the first iteration
-        t[i] = T(0);
         pc_part[i] = cvt<T>(cp);
         rhat[i] = rt;
         d[i] = T(0);
@@ -428,30 +418,23 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
     int code = kKrylovRunning;
     int it = 0;
 
-    // restart: r_hat = r, p = v = 0, s = r, t = 0 from the current residual
-    // r_of(i).  The shadow residual r_hat = b (bicgstab.rs:87) can be
-    // orthogonal to later residuals when b lives on a few source rows.
-#define OHM_RESTART(r_of)                                                      \
+    // restart: r_hat = r, p = v = 0.  The shadow residual r_hat = b
+    // (bicgstab.rs:87) can be orthogonal to later residuals when b lives on a
+    // few source rows.
+#define OHM_RESTART()                                                          \
     do {                                                                       \
         for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {              \
-            const T ri = (r_of);                                               \
             KRec<T> q = cur[i];                                                \
-            q.p = T(0); q.v = T(0); q.r = ri;                                  \
+            q.p = T(0); q.v = T(0);                                            \
             cur[i] = q;                                                        \
-            s[i] = ri;                                                         \
-            t[i] = T(0);                                                       \
-            rhat[i] = ri;                                                      \
+            rhat[i] = q.r;                                                     \
         }                                                                      \
         OHM_SYNC_OR(kKrylovAbort);                                             \
         rho = 1.0; alpha = 1.0; omega = 1.0;                                   \
         rho_new = rr_cur; rhat2 = rr_cur;                                      \
-        have_prev = false;                                                     \
         ++out.restarts;                                                        \
     } while (0)
 
-    // the previous iteration's step, applied by the owner of each row
-    bool have_prev = false;
-    double al_prev = 0.0, om_prev = 0.0;
     if (!isfinite(r0norm)) {
         code = kKrylovNan;
     } else if (r0norm < abs_tol || r0norm == 0.0) {
@@ -460,10 +443,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
         for (; it < max_it; ++it) {
             if (!(fabs(rho_new) >= kBreakdownRel * sqrt(rhat2 * rr_cur))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
-                    if (have_prev)
-                        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-                            d[i] = cvt<T>(((double)d[i] + al_prev * (double)phat[i]) + om_prev * (double)shat[i]);
-                    OHM_RESTART(cvt<T>((double)s[i] + (-omega) * (double)t[i]));
+                    OHM_RESTART();
                 } else {
                     code = kKrylovBreakRho;
                     break;
@@ -472,30 +452,26 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             const double beta = (rho_new / rho) * (alpha / omega);
             rho = rho_new;
             const double om = omega;
-            const bool hp = have_prev;
-            const double alp = al_prev, omp = om_prev;
-            // ---------------- AB: r and p on the fly, v = A M^-1 p ----------------
-            auto r_at = [&](int j) -> T { return cvt<T>((double)s[j] + (-om) * (double)t[j]); };
-            auto pnew = [&](int j, const KRec<T> &q) -> T {
-                return cvt<T>(((double)q.p + (-om) * (double)q.v) * beta + (double)r_at(j));
+            // ---------------- AB: p update and v = A M^-1 p ----------------
+            auto pnew = [&](const KRec<T> &q) -> T {
+                return cvt<T>(((double)q.p + (-om) * (double)q.v) * beta + (double)q.r);
             };
             auto phat_at = [&](int j, bool slow) -> T {
                 const KRec<T> q = cur[j];
-                double z = (double)q.c * (double)pnew(j, q);
+                double z = (double)q.c * (double)pnew(q);
                 if (slow) {
                     const int pj = partner[j];
-                    if (pj >= 0) z += (double)pc_part[j] * (double)pnew(pj, cur[pj]);
+                    if (pj >= 0) z += (double)pc_part[j] * (double)pnew(cur[pj]);
                 }
                 return cvt<T>(z);
             };
             double acc1[2] = {0.0, 0.0};
             auto ab_row = [&](int i, double y) {
-                if (hp) d[i] = cvt<T>(((double)d[i] + alp * (double)phat[i]) + omp * (double)shat[i]);
                 const KRec<T> q = cur[i];
                 KRec<T> o;
-                o.p = pnew(i, q);
+                o.p = pnew(q);
                 o.v = cvt<T>(y);
-                o.r = r_at(i);
+                o.r = q.r;
                 o.c = q.c;
                 nxt[i] = o;
                 phat[i] = phat_at(i, true);
@@ -507,10 +483,9 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             {
                 if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
             }
-            have_prev = false;                        // d now holds every step so far
             if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
-                    OHM_RESTART(nxt[i].r);            // nxt holds this iteration's r
+                    OHM_RESTART();        // cur still holds r; restart from it
                     continue;
                 }
                 code = kKrylovBreakRv;
@@ -531,29 +506,23 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 }
                 return cvt<T>(z);
             };
-            // (s,s), (t,s), (t,t), ||W s||^2, (r_hat,s), (r_hat,t), (W t, W s), ||W t||^2
-            double acc3[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            double acc3[4] = {0.0, 0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t), ||W s||^2
             auto cd_row = [&](int i, double y) {
                 const T si = s_of(nxt[i]);
                 const T ti = cvt<T>(y);
                 s[i] = si;
                 t[i] = ti;
                 shat[i] = shat_at(i, true);
-                const double wi = wt ? w[i] : 1.0;
-                const double ws = wi * (double)si, wtt = wi * (double)ti;
+                const double ws = wt ? w[i] * (double)si : (double)si;
                 acc3[0] += (double)si * (double)si;
                 acc3[1] += (double)ti * (double)si;
                 acc3[2] += (double)ti * (double)ti;
                 acc3[3] += ws * ws;
-                acc3[4] += (double)rhat[i] * (double)si;
-                acc3[5] += (double)rhat[i] * (double)ti;
-                acc3[6] += wtt * ws;
-                acc3[7] += wtt * wtt;
             };
             spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, shat_at, cd_row, a.longflag);
             if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row)) return kKrylovAbort;
             {
-                if (!g.template allreduce<8>(acc3)) return kKrylovAbort;
+                if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
             }
             if (sqrt(acc3[3]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
@@ -564,38 +533,32 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             }
             if (!(acc3[2] > 0.0)) { code = kKrylovBreakTt; break; }
             omega = acc3[1] / acc3[2];
-            { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
-            al_prev = al;
-            om_prev = omega;
-            have_prev = true;
-            // r = s - w t: its reductions from the CD ones
-            rho_new = acc3[4] - omega * acc3[5];
-            rr_cur = fmax(acc3[0] - 2.0 * omega * acc3[1] + omega * omega * acc3[2], 0.0);
-            double rnorm = sqrt(fmax(acc3[3] - 2.0 * omega * acc3[6] + omega * omega * acc3[7], 0.0));
-            if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
-            const bool last = accept_partial && it + 1 == max_it;
-            if (rnorm < abs_tol || (last && rnorm <= 0.5 * r0norm)) {
-                // confirm with the true residual
-                double tr[2] = {0.0, 0.0};   // ||W r||^2, ||r||^2
-                const double omc = omega;
-                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                    const double rt = (double)cvt<T>((double)s[i] + (-omc) * (double)t[i]);
-                    const double wr = wt ? w[i] * rt : rt;
-                    tr[0] += wr * wr;
-                    tr[1] += rt * rt;
-                }
-                if (!g.template allreduce<2>(tr)) return kKrylovAbort;
-                rnorm = sqrt(tr[0]);
-                rr_cur = tr[1];
-                if (rnorm < abs_tol || (last && rnorm <= 0.5 * r0norm)) {
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-                        d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omc * (double)shat[i]);
-                    code = kKrylovConverged;   // (an inexact last inner solve is accepted)
-                    ++it;
-                    break;
-                }
+            // ---------------- E: d, r updates ----------------
+            double acc4[3] = {0.0, 0.0, 0.0};   // (r_hat, r), ||r||^2, ||W r||^2
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omega * (double)shat[i]);
+                const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
+                nxt[i].r = rt;
+                const double wr = wt ? w[i] * (double)rt : (double)rt;
+                acc4[0] += (double)rhat[i] * (double)rt;
+                acc4[1] += (double)rt * (double)rt;
+                acc4[2] += wr * wr;
             }
+            {
+                if (!g.template allreduce<3>(acc4)) return kKrylovAbort;
+            }
+            { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
+            rho_new = acc4[0];
+            rr_cur = acc4[1];
+            const double rnorm = sqrt(acc4[2]);
+            if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
+            if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
             if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }
+            if (accept_partial && it + 1 == max_it && rnorm <= 0.5 * r0norm) {
+                code = kKrylovConverged;          // inexact inner solve accepted
+                ++it;
+                break;
+            }
         }
         if (code == kKrylovRunning) code = kKrylovMaxIter;
     }
@@ -1097,7 +1060,7 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
 // One large system per launch: the whole (co-resident) grid is the team.
 template <int LPR>
 __global__ void __launch_bounds__(kSolverBlock, 1) persistent_solver(KernelArgs a) {
-    __shared__ double smem[32 * 8 + 8];   // GridTeam reductions: warp values + results
+    __shared__ double smem[32 * 4 + 4];   // GridTeam reductions: warp values + results
     GridTeam g;
     g.G = gridDim.x;
     g.bid = blockIdx.x;

@@ -99,7 +99,7 @@ __device__ double source_value(const ohm_source &s, double t, const double *pwl)
 
 template <int LPR>
 __global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a, TranArgs T) {
-    __shared__ double smem[32 * 8 + 8];   // GridTeam reductions: warp values + results
+    __shared__ double smem[32 * 4 + 4];   // GridTeam reductions: warp values + results
     GridTeam g;
     g.G = gridDim.x;
     g.bid = blockIdx.x;
@@ -194,7 +194,7 @@ struct AdaptArgs {
 
 template <int LPR>
 __global__ void __launch_bounds__(kSolverBlock, 1) adaptive_kernel(KernelArgs a, TranArgs T, AdaptArgs P) {
-    __shared__ double smem[32 * 8 + 8];   // GridTeam reductions: warp values + results
+    __shared__ double smem[32 * 4 + 4];   // GridTeam reductions: warp values + results
     GridTeam g;
     g.G = gridDim.x;
     g.bid = blockIdx.x;
