@@ -53,10 +53,12 @@ def parse():
     p.add_argument("--tran-steps", type=int, default=2000)
     p.add_argument("--adjoint-rows", type=int, default=1000,
                    help="RC-diode mesh size of the adjoint measurement (0 skips it)")
+    p.add_argument("--ac-rows", type=int, default=100,
+                   help="RC mesh size of the AC sweep measurement (0 skips it)")
     p.add_argument("--grid-rows", type=int, default=1000,
                    help="mesh size of the large-grid DC measurement (0 skips it)")
-    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid,compile",
-                   help="comma list of dc (the headline), batch, transient, adjoint, grid, compile; a run without dc "
+    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid,compile,ac",
+                   help="comma list of dc (the headline), batch, transient, adjoint, grid, compile, ac; a run without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
     p.add_argument("--profile", choices=["fp64", "mixed", "grid"], default=None,
@@ -246,6 +248,8 @@ def main():
             line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if "compile" in sections:
             line["compile"] = compile_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "ac" in sections and args.ac_rows > 0:
+            line["ac"] = ac_section(args, S, ctx, stream, barrier, world, rank, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         plan.close()
@@ -402,6 +406,8 @@ def main():
         line["grid"] = grid_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if "compile" in sections:
         line["compile"] = compile_section(args, S, ctx, stream, barrier, world, rank, local_rank)
+    if "ac" in sections and args.ac_rows > 0:
+        line["ac"] = ac_section(args, S, ctx, stream, barrier, world, rank, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -669,6 +675,46 @@ def compile_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     res["32 Monte Carlo circuits, one call each"] = {
         "rows": int(sum(h.size for h in hs)), "host_s": t1 - t0, "device_s": t2 - t1,
         "speedup": (t1 - t0) / (t2 - t1), "bit_identical": bool(same)}
+    return res
+
+
+def ac_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """AC sweep (ac::run) of a 100x100 RC mesh (R log-uniform 10-10k ohm, C
+    log-uniform 1 fF-1 pF to ground, seed 4) driven by a 1 V AC source
+    through 50 ohm: 10 points per decade from 1 kHz to 1 THz (90 points),
+    all points in one launch through ohm_ac_sweep (host arrays in and out),
+    complex FP64 BiCGSTAB to 1e-12; the oracle's complex LU per point on a
+    sample of the points."""
+    from ohmnivore_b200 import circuits, mna
+    rows = args.ac_rows
+    ckt = circuits.rc_diode_mesh(rows, rows, seed=4, diode_frac=0.0)
+    src = int(np.flatnonzero(ckt.kind == circuits.V)[0])
+    ckt.ac[src] = (1.0, 0.0)
+    sysm = mna.compile_circuit(ckt)
+    freqs = S.ac_frequencies("dec", 10, 1e3, 1e12)
+    params = S.BiCgStabParams(max_iterations=20000, tolerance=1e-12)
+    S.ac_sweep(sysm, freqs[:4], params, ctx)                 # warm-up
+    barrier()
+    t0 = time.perf_counter()
+    x, infos = S.ac_sweep(sysm, freqs, params, ctx)
+    wall = time.perf_counter() - t0
+    its = [p["iterations"] for p in infos]
+    res = {"workload": f"AC sweep, {rows}x{rows} RC mesh ({sysm.size} rows, {sysm.g.nnz} nonzeros), "
+                       f"{len(freqs)} points 1 kHz-1 THz",
+           "value": world * len(freqs) / wall, "unit": "frequency points/s", "ms_sweep": wall * 1e3,
+           "api": "ohm_ac_sweep (host arrays; upload, one launch, download)",
+           "iterations_mean": float(np.mean(its)), "iterations_max": int(np.max(its)),
+           "failed_points": int(sum(1 for p in infos if p["status"] != 0))}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import ac_ref
+        sample = list(range(0, len(freqs), 18))
+        t0 = time.perf_counter()
+        ref = ac_ref.ac_sweep(sysm, freqs[sample])
+        cpu = time.perf_counter() - t0
+        err = max(float(np.max(np.abs(x[k] - ref[j])) / np.max(np.abs(ref[j]))) for j, k in enumerate(sample))
+        res["rel_err_vs_oracle"] = {"max": err, "points": len(sample)}
+        res["cpu_baseline"] = {"value": len(sample) / cpu, "unit": "frequency points/s", "cores": 1, "kind": "port",
+                               "sample": f"{len(sample)} of the points, complex sparse LU each, single thread"}
     return res
 
 
