@@ -20,7 +20,8 @@ using namespace ohm;
 
 namespace {
 
-constexpr int kAcBlock = 256;
+constexpr int kAcBlock = 256;       // points >> SMs: several blocks per SM
+constexpr int kAcWideBlock = 1024;  // points <= SMs on a large system: one wide block per point
 constexpr int kAcVecs = 11;        // x r rhat p v s t phat shat m_self m_part
 
 struct AcDev {
@@ -85,8 +86,8 @@ __device__ __forceinline__ void cspmv(const AcArgs &A, double w, const double2 *
     }
 }
 
-template <int LPR>
-__global__ void __launch_bounds__(kAcBlock) ac_sweep_kernel(AcArgs A) {
+template <int LPR, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
     __shared__ double smem[32 * 4];
     __shared__ int s_q;
     const int n = A.n;
@@ -261,10 +262,15 @@ __global__ void __launch_bounds__(kAcBlock) ac_sweep_kernel(AcArgs A) {
 
 using AcFn = void (*)(AcArgs);
 
-AcFn pick_ac(double avg) {
-    if (avg <= 3.0) return ac_sweep_kernel<2>;
-    if (avg <= 12.0) return ac_sweep_kernel<4>;
-    return ac_sweep_kernel<8>;
+AcFn pick_ac(double avg, bool wide) {
+    if (wide) {
+        if (avg <= 3.0) return ac_sweep_kernel<2, kAcWideBlock>;
+        if (avg <= 12.0) return ac_sweep_kernel<4, kAcWideBlock>;
+        return ac_sweep_kernel<8, kAcWideBlock>;
+    }
+    if (avg <= 3.0) return ac_sweep_kernel<2, kAcBlock>;
+    if (avg <= 12.0) return ac_sweep_kernel<4, kAcBlock>;
+    return ac_sweep_kernel<8, kAcBlock>;
 }
 
 }  // namespace
@@ -329,9 +335,12 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
     A.rp = d_rp; A.col = d_col; A.g = d_g; A.c = d_c; A.b = d_b; A.omega = d_omega;
     A.partner = d_partner; A.diag_slot = d_diag; A.off_slot = d_off;
     A.work = d_work; A.info = d_info; A.queue = d_queue;
-    AcFn fn = pick_ac((double)nnz / (double)n);
+    // a point per SM at most: give each point a whole SM when the system is large
+    const bool wide = n >= 2048 && n_freq <= c->num_sms;
+    const int block = wide ? kAcWideBlock : kAcBlock;
+    AcFn fn = pick_ac((double)nnz / (double)n, wide);
     int per_sm = 0;
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kAcBlock, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
     std::vector<double> omega(group);
     std::vector<AcDev> hinfo(group);
     int64_t failed = -1;
@@ -344,7 +353,7 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
         A.n_freq = (int)m;
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * c->num_sms, m));
         if (e == cudaSuccess) {
-            fn<<<grid, kAcBlock, 0, c->stream>>>(A);
+            fn<<<grid, block, 0, c->stream>>>(A);
             e = cudaGetLastError();
         }
         // x of every point: the first of its kAcVecs vectors

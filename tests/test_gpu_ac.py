@@ -110,3 +110,17 @@ def test_unconverged_point_is_reported():
     s = mna.compile_circuit(_rc_ladder(40, seed=1))
     with pytest.raises(S.SolveError):
         S.ac_sweep(s, [1e3, 1e6], _params(max_iterations=2))
+
+
+def test_wide_blocks_on_a_large_system():
+    """A system of >= 2048 rows swept at fewer points than SMs runs one
+    1024-thread block per point; same answers as the oracle."""
+    ckt = ck.rc_diode_mesh(50, 50, seed=4, diode_frac=0.0)
+    src = int(np.flatnonzero(ckt.kind == ck.V)[0])
+    ckt.ac[src] = (1.0, 0.0)
+    s = mna.compile_circuit(ckt)
+    assert s.size >= 2048
+    freqs = np.array([1e4, 1e7, 1e9, 3e10, 1e12])
+    x, infos = S.ac_sweep(s, freqs, _params(max_iterations=50000))
+    assert all(p["krylov_code"] == 1 for p in infos)
+    assert _err(x, ac_ref.ac_sweep(s, freqs)) < 1e-9
