@@ -120,80 +120,16 @@ __device__ __forceinline__ void block_max(double (&v)[NV], double *smem) {
     __syncthreads();
 }
 
-// Grid reduction, step 1: every block publishes its block sum to
-// partials[k * gridDim.x + blockIdx.x].
-template <int NV>
-__device__ __forceinline__ void publish_partials(double (&v)[NV], double *partials, double *smem) {
-    block_sum<NV>(v, smem);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) partials[k * gridDim.x + blockIdx.x] = v[k];
-    }
-}
-
-// Grid reduction, step 2 (after a barrier): in every block, warp k sums the
-// partials of value k in a fixed order (lane-strided, then a fixed shuffle
-// tree) and broadcasts through shared memory, so every block holds
-// bit-identical results; the NV values are gathered concurrently.
-template <int NV>
-__device__ __forceinline__ void gather_partials(const double *partials, double (&out)[NV],
-                                                double *smem) {
-    const int G = gridDim.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp < NV) {
-        const double *p = partials + (size_t)warp * G;
-        double s = 0.0;
-#pragma unroll 4
-        for (int j = lane; j < G; j += 32) s += __ldcg(p + j);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) smem[warp] = s;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = smem[k];
-    __syncthreads();
-}
-
-template <int NV>
-__device__ __forceinline__ void publish_max(double (&v)[NV], double *partials, double *smem) {
-    block_max<NV>(v, smem);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) partials[k * gridDim.x + blockIdx.x] = v[k];
-    }
-}
-
-template <int NV>
-__device__ __forceinline__ void gather_max(const double *partials, double (&out)[NV],
-                                           double *smem) {
-    const int G = gridDim.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp < NV) {
-        const double *p = partials + (size_t)warp * G;
-        double s = 0.0;
-#pragma unroll 4
-        for (int j = lane; j < G; j += 32) s = fmax(s, __ldcg(p + j));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
-        if (lane == 0) smem[warp] = s;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = smem[k];
-    __syncthreads();
-}
-
 // Grid all-reduce (sum, or max when MAX) of NV <= 4 values in one grid
 // barrier and three block synchronisations: warps reduce to shared memory;
 // warp 0 forms the block value (the same fixed tree as block_sum /
 // block_max) and its lane 0 publishes it to partials[k * G + block],
 // arrives on the barrier counter (release) and waits for every block
-// (acquire, bounded); then warp k sums the G partials of value k in a fixed
-// order and every thread reads the results.  The arithmetic is that of
-// publish_partials + grid_barrier + gather_partials, so the results are
-// bit-identical to it; `smem` holds >= 32 * 4 + 4 doubles.  Returns false
-// when the barrier wait gave up.
+// (acquire, bounded); then warp k sums the G partials of value k, lane-
+// strided in block order and then by a fixed shuffle tree, and every thread
+// reads the results.  The order is fixed, so every block holds bit-identical
+// results and repeated runs agree; `smem` holds >= 32 * 4 + 4 doubles.
+// Returns false when the barrier wait gave up.
 template <int NV, bool MAX>
 __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials, const GridSync &gs,
                                                unsigned long long &epoch, double *smem) {
@@ -258,7 +194,5 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials
     for (int k = 0; k < NV; ++k) v[k] = res[k];
     return true;
 }
-
-__device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
 }  // namespace ohm
