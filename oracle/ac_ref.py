@@ -1,8 +1,8 @@
 """ORACLE (test infrastructure only): the reference's AC sweep restated with a
 direct complex sparse LU per frequency point.
 
-Only ``tests/`` and ``bench.py``'s CPU-baseline leg may use this module, and
-only as the checker / timed CPU baseline.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use this module, and only as the checker / timed CPU baseline.
 
   ``form_complex_matrix``  A = G + j w C from triplets (src/sparse.rs:149-178)
   ``generate_frequencies`` DEC / OCT / LIN points (src/analysis/ac.rs:80-109)

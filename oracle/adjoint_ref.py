@@ -2,8 +2,8 @@
 solve or of a backward-Euler transient, by the adjoint method with a direct
 sparse LU, by FP64 forward sensitivities, and by central finite differences.
 
-Only ``tests/`` and ``bench.py``'s CPU-baseline leg may use this module, and
-only as the checker / timed CPU baseline.  The reference has no sensitivity
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use this module, and only as the checker / timed CPU baseline.  The reference has no sensitivity
 analysis; the equations are the BE companion of src/analysis/transient.rs
 (:285-333) with a Newton solve per step, written as residuals
 

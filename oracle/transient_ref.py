@@ -2,8 +2,8 @@
 source evaluation and backward-Euler companion system, with a Newton solve
 (direct sparse LU) per step.
 
-Only ``tests/`` and ``bench.py``'s CPU-baseline leg may use this module, and
-only as the checker / timed CPU baseline.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use this module, and only as the checker / timed CPU baseline.
 
   ``eval_source``   PULSE / SIN / PWL / EXP, src/analysis/transient_source.rs:8-118
   ``b_at_time``     collect_source_info + evaluate_b_at_time, transient.rs:212-280
