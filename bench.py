@@ -31,7 +31,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "solves/s & SpMV HBM GB/s: mixed-prec batched vs plain FP64 GPU at 1e-9 rel err"
-WORKLOAD = "diode-mesh 500x500 DC operating point (250,002 unknowns, 25,000 diodes, seed 1)"
+def workload(sysm, rows, cols):
+    """Name of the headline workload with its sizes (500x500: 250,002
+    unknowns, 25,000 diodes)."""
+    return (f"diode-mesh {rows}x{cols} DC operating point ({sysm.size:,} unknowns, "
+            f"{len(sysm.diode_descriptors):,} diodes, seed 1)")
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -197,7 +201,8 @@ def run_reference(args, rank):
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "newton_iterations": iters},
+            "data": "synthetic", "config": {"workload": workload(sysm, args.rows, args.cols),
+                                            "newton_iterations": iters},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
                              "sample": f"{args.steps} full DC solves of the workload (FP64 Newton + "
                                        "SuperLU per iteration, single thread); warm-up = 1 Newton "
@@ -356,7 +361,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": fp64_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "FP64 (BiCGSTAB, device eval, residual, update)",
+        "config": {"workload": workload(sysm, args.rows, args.cols),
+                   "precision": "FP64 (BiCGSTAB, device eval, residual, update)",
                    "preconditioner": "block Jacobi (2x2 for the source branch row)",
                    "newton_abs_tol": 1e-9, "krylov_tol_floor": 1e-14,
                    "inner_tolerance": "Eisenstat-Walker in [1e-4, 0.7], scaled residual",
