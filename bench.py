@@ -383,10 +383,10 @@ def main():
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,
-                     "traffic": 5.4e7 * (n / 250002.0),
+                     "traffic": 7.64e6 * (n / 40002.0),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel on the "
-                                       "200x200 mesh (8.6 MB per solve), scaled by unknowns: the working set "
-                                       "stays in L2, so DRAM sees the inputs about once per solve",
+                                       "200x200 mesh (7.64 MB per solve, 40,002 unknowns), scaled by unknowns: the "
+                                       "working set stays in L2, so DRAM sees the inputs about once per solve",
                      "peak_source": peak_src,
                      "kernel": "persistent_solver<1> (FP64 Krylov)",
                      "algorithmic_bytes_per_launch": algo_bytes,
