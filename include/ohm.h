@@ -283,6 +283,16 @@ ohm_status ohm_ac_sweep(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *ro
                         const double *freqs_hz, const ohm_krylov_params *params, double *x_re_im,
                         ohm_ac_point_info *points);
 
+/* LinearSolver::solve_complex (src/solver/mod.rs:27-34, gpu.rs:210-735):
+ * A x = b for a complex CSR matrix (values and vectors as interleaved re, im
+ * doubles), the AC sweep's complex BiCGSTAB on one point (G = Re A,
+ * C = Im A, w = 1).  Stops when ||b - A x|| < tolerance ||b||; an
+ * unconverged solve is OHM_ERR_SOLVE with info->krylov_code.  info may be
+ * NULL. */
+ohm_status ohm_solve_complex(ohm_ctx *ctx, int64_t n, int64_t nnz, const uint32_t *row_ptr, const uint32_t *col,
+                             const double *values_re_im, const double *b_re_im, double *x_re_im,
+                             const ohm_krylov_params *params, ohm_ac_point_info *info);
+
 /* -------------------------------------------------------------- transient --
  * Fixed-step backward-Euler transient with a Newton solve per step, run on
  * the device.  The reference's transient (src/analysis/transient.rs:25-210)

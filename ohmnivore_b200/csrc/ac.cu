@@ -385,3 +385,27 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
                         (long long)failed, freqs_hz[failed], fail_info.code);
     return OHM_OK;
 }
+
+// LinearSolver::solve_complex (src/solver/mod.rs:27-34, gpu.rs:210-735): one
+// complex system A x = b as a one-point sweep with G = Re A, C = Im A and
+// f = 1 / (2 pi), so that w = 2 pi f is exactly 1.0 and A(f) = A.
+extern "C" ohm_status ohm_solve_complex(ohm_ctx *c, int64_t n, int64_t nnz, const uint32_t *row_ptr,
+                                        const uint32_t *col, const double *values_re_im, const double *b_re_im,
+                                        double *x_re_im, const ohm_krylov_params *params, ohm_ac_point_info *info) {
+    if (!c || !params || n < 0 || nnz < 0) return ohm_fail(OHM_ERR_INVALID_ARG, "bad arguments");
+    if (info) std::memset(info, 0, sizeof *info);
+    if (n == 0) return OHM_OK;
+    if (!row_ptr || !b_re_im || !x_re_im || (nnz && (!col || !values_re_im)))
+        return ohm_fail(OHM_ERR_INVALID_ARG, "null array");
+    std::vector<double> re((size_t)nnz), im((size_t)nnz);
+    for (int64_t k = 0; k < nnz; ++k) {
+        re[k] = values_re_im[2 * k];
+        im[k] = values_re_im[2 * k + 1];
+    }
+    const double f = 1.0 / (2.0 * 3.14159265358979323846);
+    ohm_ac_point_info pt{};
+    const ohm_status st =
+        ohm_ac_sweep(c, n, nnz, row_ptr, col, re.data(), im.data(), b_re_im, 1, &f, params, x_re_im, &pt);
+    if (info) *info = pt;
+    return st;
+}

@@ -222,6 +222,29 @@ class GpuSolver:
             _raise(st, info)
         return x
 
+    def solve_complex(self, a, b, params: BiCgStabParams | None = None) -> np.ndarray:
+        """``LinearSolver::solve_complex`` (src/solver/gpu.rs:210-735) through
+        ``ohm_solve_complex``: complex FP64 BiCGSTAB, ||r|| < tol ||b||."""
+        n = int(a.nrows)
+        if a.ncols != n or len(b) != n:
+            raise SolveError(f"dimension mismatch: matrix is {a.nrows}x{a.ncols}, rhs length is {len(b)}")
+        if n == 0:
+            return np.zeros(0, dtype=np.complex128)
+        rp, ci = _csr_u32(a)
+        val = np.asarray(a.val, dtype=np.complex128)
+        v = np.ascontiguousarray(np.stack([val.real, val.imag], axis=1).reshape(-1))
+        bc = np.asarray(b, dtype=np.complex128)
+        bb = np.ascontiguousarray(np.stack([bc.real, bc.imag], axis=1).reshape(-1))
+        x = np.zeros(2 * n)
+        info = _lib.AcPointInfo()
+        p = (params or self.params).to_c()
+        st = self.ctx.lib.ohm_solve_complex(self.ctx.handle, n, len(ci), u32ptr(rp), u32ptr(ci), dptr(v), dptr(bb),
+                                            dptr(x), C.byref(p), C.byref(info))
+        self.last_info = info.as_dict()
+        if st != _lib.OK:
+            _raise(st, info)
+        return x[0::2] + 1j * x[1::2]
+
 
 def newton_solve(ctx, base_g_values, col_indices, row_ptrs, base_b, diode_descriptors,
                  bjt_descriptors, mosfet_descriptors, system_size, matrix_nnz,

@@ -68,3 +68,7 @@ def test_host_validation_without_gpu():
     x = np.zeros(2)
     st = lib.ohm_solve_real(None, 2, 0, None, None, None, _lib.dptr(x), _lib.dptr(x), None, None)
     assert st == _lib.ERR_INVALID_ARG
+    st = lib.ohm_solve_complex(None, 2, 0, None, None, None, _lib.dptr(x), _lib.dptr(x), None, None)
+    assert st == _lib.ERR_INVALID_ARG
+    st = lib.ohm_compile(None, 0, None, None, None, None, None)
+    assert st == _lib.ERR_INVALID_ARG
