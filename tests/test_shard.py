@@ -70,3 +70,9 @@ def test_two_gloo_ranks_shard_and_gather(tmp_path):
     expect[7] = 2
     assert np.array_equal(r0[0], expect) and np.array_equal(r1[0], expect)     # every rank sees every status
     assert not np.any(r0[1] & r1[1]) and np.all(r0[1] | r1[1])                 # disjoint shards covering all
+
+
+def test_gather_status_single_process():
+    """Without a process group the local statuses are the whole batch."""
+    full = gather_status([0, 2, 0], [4, 1, 0], 5)
+    assert full.tolist() == [0, 2, -1, -1, 0]
