@@ -61,8 +61,11 @@ def parse():
                    help="RC mesh size of the AC sweep measurement (0 skips it)")
     p.add_argument("--grid-rows", type=int, default=1000,
                    help="mesh size of the large-grid DC measurement (0 skips it)")
-    p.add_argument("--sections", default="dc,batch,transient,adjoint,grid,compile,ac",
-                   help="comma list of dc (the headline), batch, transient, adjoint, grid, compile, ac; a run without dc "
+    p.add_argument("--ladder-nodes", type=int, default=10_000,
+                   help="resistor-ladder nodes of the linear DC measurement (0 skips it)")
+    p.add_argument("--sections", default="dc,ladder,batch,transient,adjoint,grid,compile,ac",
+                   help="comma list of dc (the headline), ladder, batch, transient, adjoint, grid, compile, ac; a run "
+                        "without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
     p.add_argument("--profile", choices=["fp64", "mixed", "grid"], default=None,
@@ -81,15 +84,15 @@ def guarded(section, *args):
         return {"error": f"{type(e).__name__}: {e}"}
 
 
-def newton_params(mixed: bool):
+def newton_params(mixed: bool, precond: int = 0):
     """Newton stops at max|dx| < 1e-9 V; each linear solve is inexact with an
     Eisenstat-Walker tolerance in [1e-4, 0.7] on the diagonally scaled
     residual, above an absolute floor of 1e-14 ||W b||.  The same settings for
-    the FP64 and the mixed path."""
+    the FP64 and the mixed path; precond 0 = block Jacobi, 2 = ISAI(1)."""
     from ohmnivore_b200 import solver as S
     return S.NewtonParams(max_iterations=200, abs_tol=1e-9, bicgstab_max_iterations=20000,
                           bicgstab_tolerance=1e-14, precision=1 if mixed else 0, inner_rtol=1e-4,
-                          forcing=1, eta_max=0.7)
+                          forcing=1, eta_max=0.7, precond=precond)
 
 
 class ClockSampler:
@@ -203,7 +206,7 @@ def run_reference(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": workload(sysm, args.rows, args.cols),
                                             "newton_iterations": iters},
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "host_cores": os.cpu_count(), "kind": "port",
                              "sample": f"{args.steps} full DC solves of the workload (FP64 Newton + "
                                        "SuperLU per iteration, single thread); warm-up = 1 Newton "
                                        "iteration each"},
@@ -252,6 +255,8 @@ def main():
         line = {"metric": METRIC, "sections_only": sorted(sections)}
         if "spmv" in sections:
             line["spmv"] = spmv_roofline(S, ctx, sysm, stream, flush)
+        if "ladder" in sections and args.ladder_nodes > 0:
+            line["ladder"] = guarded(ladder_section, args, S, ctx, stream, barrier, world, rank, local_rank)
         if "batch" in sections and args.batch > 0:
             line["batch"] = guarded(batch_section, args, S, ctx, stream, barrier, world, rank, local_rank)
         if "transient" in sections and args.tran_stages > 0:
@@ -272,8 +277,8 @@ def main():
             dist.destroy_process_group()
         return
 
-    def timed_solves(mixed, steps, warmup):
-        params = newton_params(mixed)
+    def timed_solves(mixed, steps, warmup, precond=0):
+        params = newton_params(mixed, precond)
         infos = []
         for _ in range(warmup):
             with torch.cuda.stream(stream):
@@ -305,6 +310,10 @@ def main():
         fp64_ms, fp64_infos, x_fp64 = timed_solves(False, args.steps, args.warmup)
     clocks = clk.summary()
     mixed_ms, mixed_infos, x_mixed = timed_solves(True, args.steps, args.warmup)
+    # FP32 Krylov + FP64 Newton with the ISAI(1) preconditioner (the
+    # reference's choice for matrices with a zero diagonal, gpu.rs:139-168)
+    isai_steps = min(args.steps, 3)
+    isai_ms, isai_infos, x_isai = timed_solves(True, isai_steps, 1, precond=2)
 
     # ---- e2e: public C ABI, pinned host arrays, upload + solve + download ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -374,6 +383,13 @@ def main():
                             "fp64_fallbacks": mixed_infos[-1]["fp64_fallbacks"],
                             "note": "FP32 BiCGSTAB bulk; on this single L2-resident circuit the loop is "
                                     "latency-bound, so FP32 iterations cost the same as FP64 ones"},
+        "mixed_isai1": {"value": world * isai_steps / (isai_ms * 1e-3), "unit": "solves/s",
+                        "ms_per_step": isai_ms / isai_steps, "steps": isai_steps,
+                        "newton_iterations": isai_infos[-1]["iterations"],
+                        "krylov_iterations": isai_infos[-1]["krylov_iterations"],
+                        "fp64_fallbacks": isai_infos[-1]["fp64_fallbacks"],
+                        "note": "FP32 BiCGSTAB preconditioned by ISAI(1) of the device ILU(0) factors, rebuilt "
+                                "every Newton iteration; FP64 device evaluation, residual and update"},
         "mixed_vs_fp64": mixed_value / value,
         "newton_iterations": info0["iterations"], "krylov_iterations": kry,
         "krylov_restarts": info0["krylov_restarts"],
@@ -406,11 +422,14 @@ def main():
         err = lambda a, sl: float(np.max(np.abs(a[sl] - ref[sl])) / np.max(np.abs(ref[sl])))  # noqa: E731
         line["rel_err_vs_oracle"] = {
             "mixed": {"voltages": err(x_mixed, nn), "currents": err(x_mixed, br)},
+            "mixed_isai1": {"voltages": err(x_isai, nn), "currents": err(x_isai, br)},
             "fp64": {"voltages": err(x_fp64, nn), "currents": err(x_fp64, br)},
             "e2e_fp64": {"voltages": err(h_x, nn), "currents": err(h_x, br)}}
-        line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
+        line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": 1, "host_cores": os.cpu_count(), "kind": "port",
                                 "sample": f"1 full DC solve of the workload ({it_ref} FP64 Newton "
                                           "iterations, SuperLU per iteration), single thread"}
+    if "ladder" in sections and args.ladder_nodes > 0:
+        line["ladder"] = guarded(ladder_section, args, S, ctx, stream, barrier, world, rank, local_rank)
     if "batch" in sections and args.batch > 0:
         line["batch"] = guarded(batch_section, args, S, ctx, stream, barrier, world, rank, local_rank)
     if "transient" in sections and args.tran_stages > 0:
@@ -646,7 +665,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
             "mixed": float(np.max(np.abs(wave_m[:k] - ref_wave)) / np.max(np.abs(ref_wave))),
             "fp64": float(np.max(np.abs(wave_d[:k] - ref_wave)) / np.max(np.abs(ref_wave))),
             "dc_start": float(np.max(np.abs(xd[:sysm.n_nodes] - ref_dc[:sysm.n_nodes])) / 1.8)}
-        res["cpu_baseline"] = {"value": k / cpu_s, "unit": "timesteps/s", "cores": 1, "kind": "port",
+        res["cpu_baseline"] = {"value": k / cpu_s, "unit": "timesteps/s", "cores": 1, "host_cores": os.cpu_count(), "kind": "port",
                                "sample": f"{k} BE steps of the same chain, LU Newton per step, single thread"}
     tr.close()
     plan.close()
@@ -693,6 +712,96 @@ def compile_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     return res
 
 
+def ladder_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """Linear DC operating point of the 10,000-node resistor ladder (series R
+    log-uniform 100-100k ohm, shunt R 1k-1M ohm to ground, 10 V at node 1,
+    seed 0): FP64 block-Jacobi BiCGSTAB at the configured tolerance 1e-12
+    (||r|| < 1e-12 ||b||) and at 1e-13, device-resident (ohm_solve_real_device)
+    and end to end through ohm_solve_real (host arrays), each checked against
+    the oracle's dense Gaussian elimination (CpuSolver, cpu.rs:28-96) on the
+    full system.  The CPU baseline times that dense GE as the reference runs
+    it (every row update, no zero skipping) on a bounded 2,500-node ladder and
+    scales the time by (n / 2,500)^3, the operation count of the elimination."""
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    n_nodes = args.ladder_nodes
+    sysm = mna.compile_circuit(circuits.resistor_ladder(n_nodes, seed=0))
+    n, nnz = sysm.size, sysm.g.nnz
+    be = S.SolverBackend(ctx)
+    A = be.upload_matrix(sysm.g)
+    bb, bx = be.new_buffer(n), be.new_buffer(n)
+    bb.upload(sysm.b_dc)
+    reps = max(3, args.steps)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()                                     # warm-up
+        barrier()
+        ms = []
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            out = fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        barrier()
+        t = torch.tensor([sum(ms) / len(ms)], dtype=torch.float64, device=f"cuda:{local_rank}")
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), out
+
+    peaks = measured_peaks()
+    hbm_peak = peaks["hbm_gbs"] if peaks else 6650.0
+    res = {"workload": f"resistor ladder {n_nodes:,} nodes, linear DC ({n:,} rows, {nnz:,} nonzeros, seed 0)",
+           "precision": "FP64", "preconditioner": "block Jacobi (2x2 for the source branch row)"}
+    xs = {}
+    for tol in (1e-12, 1e-13):
+        params = S.BiCgStabParams(tolerance=tol, max_iterations=50000)
+        ms_dev, info = timed(lambda: be.solve_real_device(A, bb, bx, params))
+        x_dev = bx.download()
+        solver = S.GpuSolver(ctx, params)
+        ms_e2e, x_e2e = timed(lambda: solver.solve_real(sysm.g, sysm.b_dc))
+        kry = int(info["krylov_iterations"])
+        b_it = 2 * spmv_bytes(n, nnz, 8, 8) + 21 * n * 8 + 2 * n * 8
+        achieved = kry * b_it / (ms_dev * 1e-3) / 1e9
+        xs[tol] = (x_dev, x_e2e)
+        res[f"tol_{tol:g}"] = {
+            "value": world * 1e3 / ms_dev, "unit": "solves/s", "ms": ms_dev,
+            "krylov_iterations": kry, "us_per_iteration": 1e3 * ms_dev / max(kry, 1),
+            "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "ms": ms_e2e,
+                    "api": "ohm_solve_real (host CSR, b, x)",
+                    "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz + 8 * n), "d2h_bytes_per_step": int(8 * n)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak,
+                         "note": "working set ~1.4 MB, L2-resident: the loop is bound by grid synchronisation"}}
+    A.close(); bb.close(); bx.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import linear_ref
+        ref = linear_ref.dense_solve_real(n, n, sysm.g.row_ptr, sysm.g.col, sysm.g.val, sysm.b_dc)
+        nn, br = slice(0, sysm.n_nodes), slice(sysm.n_nodes, n)
+        err = lambda a, sl: float(np.max(np.abs(a[sl] - ref[sl])) / np.max(np.abs(ref[sl])))  # noqa: E731
+        for tol, (xd, xe) in xs.items():
+            res[f"tol_{tol:g}"]["rel_err_vs_dense_ge"] = {"voltages": err(xd, nn), "currents": err(xd, br),
+                                                          "e2e_voltages": err(xe, nn)}
+        m = 2500
+        small = mna.compile_circuit(circuits.resistor_ladder(m, seed=0))
+        t0 = time.perf_counter()
+        linear_ref.dense_solve_real(small.size, small.size, small.g.row_ptr, small.g.col, small.g.val,
+                                    small.b_dc, skip_zero_factors=False)
+        cpu_small = time.perf_counter() - t0
+        cpu_full = cpu_small * (n / small.size) ** 3
+        res["cpu_baseline"] = {"value": 1.0 / cpu_full, "unit": "solves/s", "cores": 1,
+                               "host_cores": os.cpu_count(), "kind": "port",
+                               "sample": f"dense GE (cpu.rs:28-96, every row update) on the {m:,}-node ladder: "
+                                         f"{cpu_small:.2f} s, scaled by ({n}/{small.size})^3 to {cpu_full:.0f} s"}
+    return res
+
+
 def ac_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     """AC sweep (ac::run) of a 100x100 RC mesh (R log-uniform 10-10k ohm, C
     log-uniform 1 fF-1 pF to ground, seed 4) driven by a 1 V AC source
@@ -729,7 +838,7 @@ def ac_section(args, S, ctx, stream, barrier, world, rank, local_rank):
         cpu = time.perf_counter() - t0
         err = max(float(np.max(np.abs(x[k] - ref[j])) / np.max(np.abs(ref[j]))) for j, k in enumerate(sample))
         res["rel_err_vs_oracle"] = {"max": err, "points": len(sample)}
-        res["cpu_baseline"] = {"value": len(sample) / cpu, "unit": "frequency points/s", "cores": 1, "kind": "port",
+        res["cpu_baseline"] = {"value": len(sample) / cpu, "unit": "frequency points/s", "cores": 1, "host_cores": os.cpu_count(), "kind": "port",
                                "sample": f"{len(sample)} of the points, complex sparse LU each, single thread"}
     return res
 
@@ -876,7 +985,7 @@ def adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank):
         lam = spl.splu(J.T.tocsc()).solve(w)
         adjoint_ref.backstamp(sysm, comps, xh, xh, lam, h)
         one = time.perf_counter() - t0
-        res["cpu_baseline"] = {"value": 1.0 / (one * (nsteps + 1)), "unit": "gradients/s", "cores": 1,
+        res["cpu_baseline"] = {"value": 1.0 / (one * (nsteps + 1)), "unit": "gradients/s", "cores": 1, "host_cores": os.cpu_count(),
                                "kind": "port", "sample": "1 reverse step (assemble J, LU of J^T, back-stamp) "
                                                          f"timed and scaled to {nsteps + 1} solves, no forward pass"}
     tr.close()

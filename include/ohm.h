@@ -109,6 +109,9 @@ typedef enum {
     OHM_FORCING_EW = 1           /* Eisenstat-Walker (choice 2), floor krylov.inner_rtol */
 } ohm_forcing;
 
+/* ohm_newton_params.continuation flag for tests of the pseudo-transient stage */
+#define OHM_CONT_TEST_PSEUDO 2
+
 typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + extensions */
     int32_t max_iterations;      /* default 50 */
     double abs_tol;              /* converged when max|x - x_old| < abs_tol (+ rel_tol*max|x|); default 1e-4 */
@@ -119,7 +122,9 @@ typedef struct {                 /* NewtonParams (src/solver/newton.rs:34-55) + 
     double eta_max;              /* Eisenstat-Walker upper bound, default 0.5 */
     int32_t continuation;        /* 1: when the direct solve fails, run the reference's DC strategy on
                                     the device (src/analysis/dc.rs:60-290): source stepping (MOSFET
-                                    circuits), GMIN stepping, pseudo-transient continuation; default 0 */
+                                    circuits), GMIN stepping, pseudo-transient continuation; default 0.
+                                    | OHM_CONT_TEST_PSEUDO (testing): the true-GMIN solve that ends GMIN
+                                    stepping counts as failed, so pseudo-transient continuation runs */
     int32_t n_nodes;             /* node rows (the first rows of the MNA system); required with
                                     continuation, which adds GMIN to their diagonals */
 } ohm_newton_params;
@@ -174,6 +179,9 @@ ohm_status ohm_csr_update_values(ohm_ctx *ctx, ohm_csr *m, const double *values,
 ohm_status ohm_csr_destroy(ohm_csr *m);
 ohm_status ohm_spmv(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *x, ohm_buf *y);       /* spmv */
 ohm_status ohm_dot(ohm_ctx *ctx, const ohm_buf *a, const ohm_buf *b, double *out);      /* dot -> f64 */
+/* dot_n (backend.rs:60-68): x . y over the first n entries only (the owned
+ * rows of a buffer that also holds halo entries); n <= both lengths. */
+ohm_status ohm_dot_n(ohm_ctx *ctx, const ohm_buf *a, const ohm_buf *b, int64_t n, double *out);
 ohm_status ohm_axpy(ohm_ctx *ctx, double alpha, const ohm_buf *x, ohm_buf *y);          /* y += a x */
 ohm_status ohm_copy(ohm_ctx *ctx, const ohm_buf *src, ohm_buf *dst);                    /* copy */
 ohm_status ohm_scale(ohm_ctx *ctx, double alpha, ohm_buf *x);                            /* scale */
@@ -210,7 +218,9 @@ ohm_status ohm_solve_real_device(ohm_ctx *ctx, const ohm_csr *a, const ohm_buf *
  * with OHM_ERR_INVALID_ARG.  The first call on a device looks up that
  * device's address of the array: make it before any stream capture.  Every
  * call shares the array, so calls that overlap on the GPU race; x and all
- * state that must start at zero are cleared by each call. */
+ * state that must start at zero are cleared by each call.  Each call
+ * synchronises the stream (it reads the CSR check back before the solve and
+ * the status after it) and returns when the solve has finished. */
 ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nnz, const uint32_t *d_row_ptr,
                                   const uint32_t *d_col, const double *d_values, const double *d_b,
                                   double *d_x, const ohm_krylov_params *params, ohm_solve_info *info);
@@ -399,13 +409,16 @@ ohm_status ohm_transient_run_adaptive(ohm_transient *tr, double *x_inout_device,
 
 /* ---------------------------------------------------------------- adjoint --
  * Sensitivities of one output o = w . x (w = do/dx, host, size n) with
- * respect to every resistance, capacitance and diode saturation current, by
- * the adjoint method; no counterpart in the reference.
+ * respect to every resistance, capacitance, diode saturation current and
+ * MOSFET threshold |VTO| and transconductance KP, by the adjoint method; no
+ * counterpart in the reference.
  *
  * DC: J(x)^T lambda = w at the operating point x (the BiCGSTAB of this
  * library on the transposed CSR), then do/dp = -lambda^T dF/dp, back-stamped
  * per component: resistor (a, b, R): (v_a - v_b)(lambda_a - lambda_b) / R^2;
- * diode: -(lambda_anode - lambda_cathode)(exp(v / nVt) - 1).
+ * diode: -(lambda_anode - lambda_cathode)(exp(v / nVt) - 1); MOSFET (drain
+ * current i_d at x, g_m = di_d/dV_GS): d/d|VTO| = (lambda_D - lambda_S) pol g_m,
+ * d/dKP = -(lambda_D - lambda_S) i_d / KP.
  *
  * Transient (backward Euler, F_n = (G + C/h) x_n - (C/h) x_{n-1} + i(x_n)
  * - b(t_n), o = w . x_N): J_N^T lambda_N = w, J_n^T lambda_n = (C/h)^T
@@ -435,20 +448,25 @@ typedef struct {
 } ohm_adjoint_info;
 
 /* DC adjoint at the operating point x_dev (device).  Gradient outputs (host,
- * may be NULL): d_out_dr[n_resistors], d_out_dis[plan's diodes];
+ * may be NULL): d_out_dr[n_resistors], d_out_dis[plan's diodes],
+ * d_out_dvto[plan's MOSFETs] (with respect to the descriptor's |VTO|, the
+ * threshold magnitude the model uses), d_out_dkp[plan's MOSFETs] (with
+ * respect to the descriptor's KP, i.e. KP W/L where W/L is folded in);
  * lambda_host (may be NULL) receives lambda.  kp: FP64 Krylov settings. */
 ohm_status ohm_plan_adjoint_dc(ohm_plan *plan, const double *x_dev, const double *w_host,
                                const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
-                               double *d_out_dis, double *lambda_host, ohm_adjoint_info *info);
+                               double *d_out_dis, double *d_out_dvto, double *d_out_dkp, double *lambda_host,
+                               ohm_adjoint_info *info);
 /* Transient adjoint: forward n_steps BE steps from x0_dev (the DC operating
  * point at t0, left unchanged) with Newton params np, then the reverse
  * sweep.  Outputs (host, may be NULL): d_out_dr, d_out_dc[n_capacitors],
- * d_out_dis.  Includes the dependence of x0 on the parameters (the DC
- * adjoint at the start). */
+ * d_out_dis, d_out_dvto, d_out_dkp (as for the DC adjoint).  Includes the
+ * dependence of x0 on the parameters (the DC adjoint at the start). */
 ohm_status ohm_transient_adjoint(ohm_transient *tr, const double *x0_dev, double t0, double h, int32_t n_steps,
                                  int32_t checkpoint_every, const ohm_newton_params *np, const double *w_host,
                                  const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
-                                 double *d_out_dc, double *d_out_dis, ohm_adjoint_info *info);
+                                 double *d_out_dc, double *d_out_dis, double *d_out_dvto, double *d_out_dkp,
+                                 ohm_adjoint_info *info);
 
 /* ---------------------------------------------------------------- batches --
  * Many independent nonlinear circuits solved by one launch (Monte Carlo

@@ -18,6 +18,7 @@ OK, ERR_SOLVE, ERR_NEWTON_NOT_CONVERGED, ERR_NEWTON_NUMERICAL, ERR_COMPILE, ERR_
     ERR_INVALID_ARG, ERR_CUDA, ERR_TIMESTEP = range(9)
 PREC_FP64, PREC_MIXED = 0, 1
 PRECOND_AUTO, PRECOND_JACOBI, PRECOND_ISAI1, PRECOND_NONE = 0, 1, 2, 3
+CONT_ON, CONT_TEST_PSEUDO = 1, 2   # ohm_newton_params.continuation bits
 
 
 class KrylovParams(C.Structure):
@@ -124,6 +125,7 @@ SIGNATURES = {
     "ohm_csr_destroy": (C.c_int, [_vp]),
     "ohm_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ohm_dot": (C.c_int, [_vp, _vp, _vp, _dp]),
+    "ohm_dot_n": (C.c_int, [_vp, _vp, _vp, _i64, _dp]),
     "ohm_axpy": (C.c_int, [_vp, C.c_double, _vp, _vp]),
     "ohm_copy": (C.c_int, [_vp, _vp, _vp]),
     "ohm_scale": (C.c_int, [_vp, C.c_double, _vp]),
@@ -151,10 +153,10 @@ SIGNATURES = {
                                        C.c_int32, C.POINTER(_vp)]),
     "ohm_transient_destroy": (C.c_int, [_vp]),
     "ohm_plan_adjoint_dc": (C.c_int, [_vp, _vp, _dp, C.POINTER(Components), C.POINTER(KrylovParams), _dp, _dp, _dp,
-                                      C.POINTER(AdjointInfo)]),
+                                      _dp, _dp, C.POINTER(AdjointInfo)]),
     "ohm_transient_adjoint": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                         C.POINTER(NewtonParamsC), _dp, C.POINTER(Components),
-                                        C.POINTER(KrylovParams), _dp, _dp, _dp, C.POINTER(AdjointInfo)]),
+                                        C.POINTER(KrylovParams), _dp, _dp, _dp, _dp, _dp, C.POINTER(AdjointInfo)]),
     "ohm_ac_sweep": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, _i64, _dp, C.POINTER(KrylovParams),
                                _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,

@@ -742,7 +742,7 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
     a.trace = p->trace;
     a.trace_cap = kTraceRows;
-    a.continuation = np->continuation ? 1 : 0;
+    a.continuation = np->continuation ? (1 | (np->continuation & OHM_CONT_TEST_PSEUDO)) : 0;
     a.n_nodes = (int)std::min<int64_t>(np->n_nodes, p->n);
     a.stampflag = p->stampflag;
     a.x_good = p->x_good;

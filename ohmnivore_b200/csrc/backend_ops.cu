@@ -197,16 +197,30 @@ extern "C" ohm_status ohm_spmv(ohm_ctx *c, const ohm_csr *a, const ohm_buf *x, o
     return OHM_OK;
 }
 
-extern "C" ohm_status ohm_dot(ohm_ctx *c, const ohm_buf *a, const ohm_buf *b, double *out) {
-    if (!c || !a || !b || !out) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
-    if (a->n != b->n) return ohm_fail(OHM_ERR_INVALID_ARG, "dot length mismatch");
-    const int grid = std::min(grid_for(a->n), 1024);
-    dot_partial_kernel<<<grid, kOpsBlock, 0, c->stream>>>(a->n, a->d, b->d, c->dot_scratch);
+// x . y over the first n entries: per-block partials, then one block sums
+// them in a fixed order (the same result for the same inputs every call).
+static ohm_status dot_first(ohm_ctx *c, const ohm_buf *a, const ohm_buf *b, int64_t n, double *out) {
+    const int grid = std::min(grid_for(n), 1024);
+    dot_partial_kernel<<<grid, kOpsBlock, 0, c->stream>>>(n, a->d, b->d, c->dot_scratch);
     dot_final_kernel<<<1, 1024, 0, c->stream>>>(grid, c->dot_scratch, c->dot_scratch + 2040);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, c->dot_scratch + 2040, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return OHM_OK;
+}
+
+extern "C" ohm_status ohm_dot(ohm_ctx *c, const ohm_buf *a, const ohm_buf *b, double *out) {
+    if (!c || !a || !b || !out) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (a->n != b->n) return ohm_fail(OHM_ERR_INVALID_ARG, "dot length mismatch");
+    return dot_first(c, a, b, a->n, out);
+}
+
+extern "C" ohm_status ohm_dot_n(ohm_ctx *c, const ohm_buf *a, const ohm_buf *b, int64_t n, double *out) {
+    if (!c || !a || !b || !out) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
+    if (n < 0 || n > a->n || n > b->n)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "dot_n: n = %lld outside the buffers (%lld, %lld)", (long long)n,
+                        (long long)a->n, (long long)b->n);
+    return dot_first(c, a, b, n, out);
 }
 
 extern "C" ohm_status ohm_axpy(ohm_ctx *c, double alpha, const ohm_buf *x, ohm_buf *y) {

@@ -258,7 +258,7 @@ static ohm_status batch_args(ohm_batch *b, double *x_dev, const ohm_newton_param
     a.fp32_max_iterations = np->krylov.fp32_max_iterations > 0 ? np->krylov.fp32_max_iterations
                                                                : np->krylov.max_iterations;
     a.max_restarts = std::max(0, np->krylov.max_restarts);
-    a.continuation = np->continuation ? 1 : 0;
+    a.continuation = np->continuation ? (1 | (np->continuation & OHM_CONT_TEST_PSEUDO)) : 0;
     return OHM_OK;
 }
 

@@ -115,8 +115,15 @@ __device__ __forceinline__ void bjt_stamps(const BjtDesc &q, double vaf, const d
     rs[0] = -(ic - ilc); rs[1] = -(ibp - ilb); rs[2] = -(ie - ile);
 }
 
-__device__ __forceinline__ void mosfet_stamps(const MosfetDesc &m, const double *x, double *ms,
-                                              double *rs) {
+// MOSFET drain current at x (ds_nonlinear_shaders.rs:746-849): i_d with the
+// polarity applied, g_m = dI/dV_GS and g_ds = dI/dV_DS (polarity-free), and
+// i_per_kp = i_d / KP (the current is linear in KP), plus the terminal
+// voltages.  d i_d / d|VTO| = -polarity * g_m.
+struct MosEval {
+    double i_d, gm, gds, i_per_kp, vd, vg, vs;
+};
+
+__device__ __forceinline__ MosEval mosfet_eval(const MosfetDesc &m, const double *x) {
     const double pol = (double)m.polarity, vto = (double)m.vto;
     const double kp = (double)m.kp, lam = (double)m.lambda;
     const double vd = node_v(x, m.drain), vg = node_v(x, m.gate), vs = node_v(x, m.source);
@@ -134,20 +141,28 @@ __device__ __forceinline__ void mosfet_stamps(const MosfetDesc &m, const double 
         sig = 1.0 / (1.0 + exp(-arg));
     }
     const double lamf = 1.0 + lam * vds;
-    double i_d, gm, gds;
+    double i_d, gm, gds, ipk;
     if (vds < veff) {                      // linear region
         const double inner = veff * vds - 0.5 * (vds * vds);
         const double kp_inner = kp * inner;
         i_d = kp_inner * lamf;
         gm = (kp * vds) * lamf * sig;
         gds = (kp * (veff - vds)) * lamf + kp_inner * lam;
+        ipk = inner * lamf;
     } else {                               // saturation
         const double kh_vov2 = (kp / 2.0) * (veff * veff);
         i_d = kh_vov2 * lamf;
         gm = (kp * veff) * lamf * sig;
         gds = kh_vov2 * lam;
+        ipk = 0.5 * (veff * veff) * lamf;
     }
-    i_d *= pol;
+    return MosEval{i_d * pol, gm, gds, ipk * pol, vd, vg, vs};
+}
+
+__device__ __forceinline__ void mosfet_stamps(const MosfetDesc &m, const double *x, double *ms,
+                                              double *rs) {
+    const MosEval ev = mosfet_eval(m, x);
+    const double i_d = ev.i_d, gm = ev.gm, gds = ev.gds, vd = ev.vd, vg = ev.vg, vs = ev.vs;
     const double s = gm + gds;
     ms[0] = gds; ms[1] = gm; ms[2] = -s; ms[3] = -gds; ms[4] = -gm; ms[5] = s;
     const double ild = (gds * vd + gm * vg) + (-s) * vs;

@@ -15,6 +15,8 @@
 // before any stream capture.  Every call shares the array and leaves its
 // contents behind; everything that must start at zero is cleared per call.
 // Calls that overlap on the GPU (two streams, two threads) race on the array.
+// Each call blocks the host: it reads the CSR check flag back before the solve
+// and the solve's status after it, synchronising the stream both times.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -204,17 +206,18 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
 
     const bool mixed = params->precision == OHM_PREC_MIXED;
     int launches = 1;
-    if (params->precond == OHM_PRECOND_AUTO || params->precond == OHM_PRECOND_JACOBI) {
-        pc_diag_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, diag, partner, off, cand, choice);
-        launches += 1;
-        if (params->precond == OHM_PRECOND_AUTO) {
-            pc_choose_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, d_values, diag, cand, choice);
-            pc_pair_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, cand, choice, partner, off);
-            pc_flag_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, partner, rowflag);
-            launches += 3;
-        }
-    } else {
-        CUDA_TRY(cudaMemsetAsync(partner, 0xFF, n * sizeof(int32_t), s));   // -1: unpaired
+    // The diagonal-slot table is rebuilt on every call, whatever the
+    // preconditioner: the solver reads it for every row (the Jacobi
+    // coefficient, or nothing but the sentinel check), and a table left by an
+    // earlier, larger system would index past this call's values.  It also
+    // resets partner to -1 (unpaired).
+    pc_diag_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, diag, partner, off, cand, choice);
+    launches += 1;
+    if (params->precond == OHM_PRECOND_AUTO) {
+        pc_choose_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, d_values, diag, cand, choice);
+        pc_pair_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, cand, choice, partner, off);
+        pc_flag_kernel<<<small_grid(n), 256, 0, s>>>((int)n, d_row_ptr, d_col, partner, rowflag);
+        launches += 3;
     }
     CUDA_TRY(cudaGetLastError());
     if (mixed) {
@@ -254,6 +257,9 @@ extern "C" ohm_status ohm_solve_real_noalloc(void *stream, int64_t n, int64_t nn
     a.inner_rtol = mixed ? (params->inner_rtol > 0.0 ? params->inner_rtol : 1e-4) : params->inner_rtol;
     a.require_true_residual = params->max_refinements > 1 ? 1 : 0;
     a.max_restarts = std::max(0, params->max_restarts);
+    // the same FP32 attempt cap and forcing bound as ohm_solve_real
+    a.fp32_max_iterations = params->fp32_max_iterations > 0 ? params->fp32_max_iterations : params->max_iterations;
+    a.eta_max = 0.5;
 
     DeviceInfo host_info;
     std::memset(&host_info, 0, sizeof host_info);

@@ -138,9 +138,10 @@ struct KernelArgs {
     const uint8_t *lseg_flag;    // per mslot/rrow entry: 1 if handled as a long segment
     double *lseg_part;
 
-    // DC continuation (src/analysis/dc.rs): 1 = on failure of the direct
+    // DC continuation (src/analysis/dc.rs): bit 0 = on failure of the direct
     // Newton solve, run source stepping (MOSFET circuits), GMIN stepping and
-    // pseudo-transient continuation on the device.  n_nodes: node rows come
+    // pseudo-transient continuation on the device; bit 1 (testing) = treat
+    // the true-GMIN solve after GMIN stepping as failed.  n_nodes: node rows come
     // first (MNA order).  stampflag per row: bit 0 = its diagonal slot is
     // written by the stamp map, bit 1 = its rhs entry is.  x_good: last
     // converged continuation point (size n).
@@ -1008,7 +1009,9 @@ __device__ __forceinline__ bool solve_body(const KernelArgs &a, Team &g, DeviceI
                 }
                 break;
             case kGminFinal:
-                if (ok || !have_good) { finished = true; break; }
+                // continuation bit 1 (testing): count this solve as failed so
+                // that the pseudo-transient stage runs
+                if ((ok && !(a.continuation & 2)) || !have_good) { finished = true; break; }
                 stage = kPseudo; kind = kContPseudo; last = 1.0; target = 1e-1; subdiv = 0;
                 xsrc = 1;
                 c = RunCfg{target, 1.0, target, 20, cont_cap(a, 500), false};

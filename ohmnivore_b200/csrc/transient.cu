@@ -867,19 +867,23 @@ namespace {
 struct BackArgs {
     const double *x, *xprev, *lam;     // xprev null: DC (no capacitor term)
     double inv_h;
-    int64_t nr, nc, nd;
+    int64_t nr, nc, nd, nm;
     const int32_t *ra, *rb, *ca, *cb;
     const double *rv, *cv;
     const DiodeDesc *dio;
-    double *gr, *gc, *gd;
+    const MosfetDesc *mos;
+    double *gr, *gc, *gd, *gvto, *gkp;
 };
 
 __device__ __forceinline__ double at(const double *v, int32_t i) { return i >= 0 ? v[i] : 0.0; }
 
 // do/dp += -lambda^T dF/dp for every component, one thread per component
-// (accumulation over steps in launch order: deterministic).
+// (accumulation over steps in launch order: deterministic).  A device current
+// i enters F at its first terminal and leaves at its second, so a parameter p
+// of it contributes -(lambda_1 - lambda_2) di/dp: diode di/dIs = exp(v/nVt) - 1;
+// MOSFET (drain, source) di/d|VTO| = -polarity g_m, di/dKP = i / KP.
 __global__ void backstamp_kernel(BackArgs B) {
-    const int64_t total = B.nr + (B.xprev ? B.nc : 0) + B.nd;
+    const int64_t total = B.nr + (B.xprev ? B.nc : 0) + B.nd + B.nm;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
         if (k < B.nr) {
             const int32_t a = B.ra[k], b = B.rb[k];
@@ -897,10 +901,19 @@ __global__ void backstamp_kernel(BackArgs B) {
             }
             q -= B.nc;
         }
-        const DiodeDesc &d = B.dio[q];
-        const double v = node_v(B.x, d.anode) - node_v(B.x, d.cathode);
-        const double e = clamp_exp(v / (double)d.n_vt);
-        B.gd[q] -= (node_v(B.lam, d.anode) - node_v(B.lam, d.cathode)) * (e - 1.0);
+        if (q < B.nd) {
+            const DiodeDesc &d = B.dio[q];
+            const double v = node_v(B.x, d.anode) - node_v(B.x, d.cathode);
+            const double e = clamp_exp(v / (double)d.n_vt);
+            B.gd[q] -= (node_v(B.lam, d.anode) - node_v(B.lam, d.cathode)) * (e - 1.0);
+            continue;
+        }
+        q -= B.nd;
+        const MosfetDesc &m = B.mos[q];
+        const MosEval ev = mosfet_eval(m, B.x);
+        const double dl = node_v(B.lam, m.drain) - node_v(B.lam, m.source);
+        B.gvto[q] += dl * ((double)m.polarity * ev.gm);
+        B.gkp[q] -= dl * ev.i_per_kp;
     }
 }
 
@@ -994,7 +1007,7 @@ struct AdjointCtx {
         int32_t *i32 = nullptr;
         double *f64 = nullptr;
         B = BackArgs{};
-        B.nr = nr; B.nc = nc; B.nd = a.nd; B.dio = a.diodes;
+        B.nr = nr; B.nc = nc; B.nd = a.nd; B.dio = a.diodes; B.nm = a.nm; B.mos = a.mosfets;
         if (e == cudaSuccess && nr) { e = put(&i32, comps->r_a, nr); B.ra = i32; }
         if (e == cudaSuccess && nr) { e = put(&i32, comps->r_b, nr); B.rb = i32; }
         if (e == cudaSuccess && nr) { e = put(&f64, comps->r_ohms, nr); B.rv = f64; }
@@ -1004,6 +1017,8 @@ struct AdjointCtx {
         if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(nr, 1)); B.gr = f64; }
         if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(nc, 1)); B.gc = f64; }
         if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(a.nd, 1)); B.gd = f64; }
+        if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(a.nm, 1)); B.gvto = f64; }
+        if (e == cudaSuccess) { e = put(&f64, (const double *)nullptr, std::max<int64_t>(a.nm, 1)); B.gkp = f64; }
         if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "adjoint set-up: %s", cudaGetErrorString(e));
         B.lam = lam;
         return OHM_OK;
@@ -1024,14 +1039,16 @@ struct AdjointCtx {
         b.x = x;
         b.xprev = xprev;
         b.inv_h = inv_h;
-        const int64_t total = b.nr + (xprev ? b.nc : 0) + b.nd;
+        const int64_t total = b.nr + (xprev ? b.nc : 0) + b.nd + b.nm;
         if (total) backstamp_kernel<<<steps_grid(total), 256, 0, c->stream>>>(b);
         CUDA_TRY(cudaGetLastError());
         return OHM_OK;
     }
 
-    ohm_status download(double *gr, double *gc, double *gd, double *lam_host) {
+    ohm_status download(double *gr, double *gc, double *gd, double *gvto, double *gkp, double *lam_host) {
         if (gr && B.nr) CUDA_TRY(cudaMemcpyAsync(gr, B.gr, B.nr * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (gvto && B.nm) CUDA_TRY(cudaMemcpyAsync(gvto, B.gvto, B.nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (gkp && B.nm) CUDA_TRY(cudaMemcpyAsync(gkp, B.gkp, B.nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         if (gc && B.nc) CUDA_TRY(cudaMemcpyAsync(gc, B.gc, B.nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         if (gd && B.nd) CUDA_TRY(cudaMemcpyAsync(gd, B.gd, B.nd * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         if (lam_host) CUDA_TRY(cudaMemcpyAsync(lam_host, lam, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1054,7 +1071,8 @@ double host_dot(ohm_ctx *c, const double *w, const double *x_dev, int64_t n) {
 
 extern "C" ohm_status ohm_plan_adjoint_dc(ohm_plan *plan, const double *x_dev, const double *w_host,
                                           const ohm_components *comps, const ohm_krylov_params *kp, double *d_out_dr,
-                                          double *d_out_dis, double *lambda_host, ohm_adjoint_info *info) {
+                                          double *d_out_dis, double *d_out_dvto, double *d_out_dkp,
+                                          double *lambda_host, ohm_adjoint_info *info) {
     if (!plan || !x_dev || !w_host || !kp) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
     ohm_newton_params np;
     ohm_newton_params_default(&np);
@@ -1069,7 +1087,7 @@ extern "C" ohm_status ohm_plan_adjoint_dc(ohm_plan *plan, const double *x_dev, c
     CUDA_TRY(cudaMemcpyAsync(A.rhs, w_host, a.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     int64_t kiters = 0;
     st = A.step(plan, x_dev, nullptr, nullptr, 0.0, kp, kiters);
-    if (st == OHM_OK) st = A.download(d_out_dr, nullptr, d_out_dis, lambda_host);
+    if (st == OHM_OK) st = A.download(d_out_dr, nullptr, d_out_dis, d_out_dvto, d_out_dkp, lambda_host);
     if (info) {
         std::memset(info, 0, sizeof *info);
         info->status = st;
@@ -1084,7 +1102,8 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
                                             int32_t n_steps, int32_t checkpoint_every, const ohm_newton_params *np,
                                             const double *w_host, const ohm_components *comps,
                                             const ohm_krylov_params *kp, double *d_out_dr, double *d_out_dc,
-                                            double *d_out_dis, ohm_adjoint_info *info) {
+                                            double *d_out_dis, double *d_out_dvto, double *d_out_dkp,
+                                            ohm_adjoint_info *info) {
     if (!t || !x0_dev || !np || !w_host || !kp) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
     if (!(h > 0.0) || n_steps < 1 || checkpoint_every < 1)
         return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 1, checkpoint_every >= 1");
@@ -1193,7 +1212,7 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
         if (st != OHM_OK) st = ohm_fail(st, "adjoint solve of the DC start: %s", ohm_last_error());
     }
     restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
-    if (st == OHM_OK) st = A.download(d_out_dr, d_out_dc, d_out_dis, nullptr);
+    if (st == OHM_OK) st = A.download(d_out_dr, d_out_dc, d_out_dis, d_out_dvto, d_out_dkp, nullptr);
     if (info) {
         std::memset(info, 0, sizeof *info);
         info->status = st;

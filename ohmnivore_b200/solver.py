@@ -123,7 +123,8 @@ class NewtonParams:
     forcing: int = 0              # 0 constant inner_rtol, 1 Eisenstat-Walker
     eta_max: float = 0.5
     fp32_max_iterations: int = 600
-    continuation: bool = False    # reference DC strategy on failure (src/analysis/dc.rs:60-290)
+    continuation: int = 0         # 1: reference DC strategy on failure (src/analysis/dc.rs:60-290);
+                                  # | CONT_TEST_PSEUDO (testing): force the pseudo-transient stage
     n_nodes: int = 0              # node rows; filled from the system by NewtonPlan / NewtonBatch
 
     def to_c(self):
@@ -137,7 +138,7 @@ class NewtonParams:
                                   fp32_max_iterations=self.fp32_max_iterations).to_c()
         p.forcing = int(self.forcing)
         p.eta_max = float(self.eta_max)
-        p.continuation = 1 if self.continuation else 0
+        p.continuation = int(self.continuation)
         p.n_nodes = int(self.n_nodes)
         keep = None
         if self.initial_guess is not None:
@@ -569,20 +570,24 @@ class ComponentTable:
 
 def adjoint_dc(plan: "NewtonPlan", x_dev_ptr: int, w, comps: ComponentTable, params: BiCgStabParams | None = None):
     """do/dp of o = w . x at the DC operating point x (device pointer) for
-    every resistor and diode Is.  Returns (dict of gradients, lambda, info)."""
+    every resistor, diode Is and MOSFET |VTO| and KP (the descriptor values:
+    the threshold magnitude, and KP with W/L folded in).
+    Returns (dict of gradients, lambda, info)."""
     kp = (params or BiCgStabParams(max_iterations=20000, tolerance=1e-14)).to_c()
     w = np.ascontiguousarray(w, dtype=np.float64)
     gr = np.zeros(len(comps.r_ohms))
     gd = np.zeros(len(plan.sysm.diode_descriptors))
+    nm = len(plan.sysm.mosfet_descriptors)
+    gvto, gkp = np.zeros(nm), np.zeros(nm)
     lam = np.zeros(plan.n)
     info = _lib.AdjointInfo()
     cc = comps.to_c()
+    opt = lambda a: dptr(a) if len(a) else None   # noqa: E731
     st = plan.ctx.lib.ohm_plan_adjoint_dc(plan._h, C.c_void_p(int(x_dev_ptr)), dptr(w), C.byref(cc), C.byref(kp),
-                                          dptr(gr) if len(gr) else None, dptr(gd) if len(gd) else None, dptr(lam),
-                                          C.byref(info))
+                                          opt(gr), opt(gd), opt(gvto), opt(gkp), dptr(lam), C.byref(info))
     if st != _lib.OK:
         _raise(st)
-    return {"R": gr, "Is": gd}, lam, info.as_dict()
+    return {"R": gr, "Is": gd, "VTO": gvto, "KP": gkp}, lam, info.as_dict()
 
 
 def compile_circuit_device(ckt, ctx: Context | None = None) -> "mna.MnaSystem":
@@ -713,26 +718,28 @@ class Transient:
     def adjoint(self, x0_dev_ptr: int, t0: float, h: float, n_steps: int, w, comps: ComponentTable,
                 params: NewtonParams | None = None, checkpoint_every: int = 50,
                 krylov: BiCgStabParams | None = None):
-        """do/dp of o = w . x(t0 + n_steps h) for every resistor, capacitor and
-        diode Is (the DC start x0 included).  x0 is left unchanged.
-        Returns (dict of gradients, info)."""
+        """do/dp of o = w . x(t0 + n_steps h) for every resistor, capacitor,
+        diode Is and MOSFET |VTO| and KP (the DC start x0 included).  x0 is
+        left unchanged.  Returns (dict of gradients, info)."""
         p, keep = (params or NewtonParams()).to_c()
         kp = (krylov or BiCgStabParams(max_iterations=20000, tolerance=1e-14)).to_c()
         w = np.ascontiguousarray(w, dtype=np.float64)
         gr = np.zeros(len(comps.r_ohms))
         gc = np.zeros(len(comps.c_farads))
         gd = np.zeros(len(self.plan.sysm.diode_descriptors))
+        nm = len(self.plan.sysm.mosfet_descriptors)
+        gvto, gkp = np.zeros(nm), np.zeros(nm)
         info = _lib.AdjointInfo()
         cc = comps.to_c()
+        opt = lambda a: dptr(a) if len(a) else None   # noqa: E731
         st = self.ctx.lib.ohm_transient_adjoint(self._h, C.c_void_p(int(x0_dev_ptr)), float(t0), float(h),
                                                 int(n_steps), int(checkpoint_every), C.byref(p), dptr(w),
-                                                C.byref(cc), C.byref(kp), dptr(gr) if len(gr) else None,
-                                                dptr(gc) if len(gc) else None, dptr(gd) if len(gd) else None,
-                                                C.byref(info))
+                                                C.byref(cc), C.byref(kp), opt(gr), opt(gc), opt(gd), opt(gvto),
+                                                opt(gkp), C.byref(info))
         del keep
         if st != _lib.OK:
             _raise(st)
-        return {"R": gr, "C": gc, "Is": gd}, info.as_dict()
+        return {"R": gr, "C": gc, "Is": gd, "VTO": gvto, "KP": gkp}, info.as_dict()
 
     def run(self, x_dev_ptr: int, t0: float, h: float, n_steps: int, params: NewtonParams | None = None,
             steps_per_launch: int = 100, graph: bool = True, check: bool = True):
@@ -862,6 +869,12 @@ class SolverBackend:
     def dot(self, a: DeviceBuffer, b: DeviceBuffer) -> float:
         out = C.c_double()
         self._chk(self.ctx.lib.ohm_dot(self.ctx.handle, a._h, b._h, C.byref(out)))
+        return out.value
+
+    def dot_n(self, a: DeviceBuffer, b: DeviceBuffer, n: int) -> float:
+        """``dot_n`` (backend.rs:60-68): the dot product over the first n entries."""
+        out = C.c_double()
+        self._chk(self.ctx.lib.ohm_dot_n(self.ctx.handle, a._h, b._h, int(n), C.byref(out)))
         return out.value
 
     def axpy(self, alpha, x, y):

@@ -11,8 +11,11 @@ analysis; the equations are the BE companion of src/analysis/transient.rs
     F_n(x_n) = (G + C/h) x_n - (C/h) x_{n-1} + i(x_n) - b(t_n)
 
 for an output o = w . x_N.  Parameters: every resistance R (conductance 1/R
-between its terminals), capacitance C and diode saturation current Is
-(i_d = Is (exp(v / nVt) - 1), the stored f32 value).
+between its terminals), capacitance C, diode saturation current Is
+(i_d = Is (exp(v / nVt) - 1), the stored f32 value), and every MOSFET's
+threshold magnitude |VTO| and transconductance KP (the descriptor values;
+the drain current of ds_nonlinear_shaders.rs:746-849 depends on them through
+v_ov = V_GS - |VTO| and linearly on KP).
 """
 from __future__ import annotations
 
@@ -49,8 +52,22 @@ def _diode_terms(sysm, x):
     return an, ca, e - 1.0
 
 
+def _mosfet_terms(sysm, x):
+    """Drain/source rows (-1 = ground), dI/d|VTO| and dI/dKP of the drain
+    current I (polarity applied) at x."""
+    m = sysm.mosfet_descriptors
+    dr = m["drain"].astype(np.int64)
+    so = m["source"].astype(np.int64)
+    dr = np.where(dr == 0xFFFFFFFF, -1, dr)
+    so = np.where(so == 0xFFFFFFFF, -1, so)
+    i_d, g_m, _ = dev.mosfet_eval(m, x)
+    pol = m["polarity"].astype(np.float64)
+    return dr, so, -pol * g_m, i_d / m["kp"].astype(np.float64)
+
+
 def backstamp(sysm, comps, x, xprev, lam, h):
-    """-lambda^T dF/dp per component (xprev None: the DC equation)."""
+    """-lambda^T dF/dp per component (xprev None: the DC equation); MOSFET
+    gradients are returned by ``backstamp_mosfets``."""
     dv = _at(x, comps.r_a) - _at(x, comps.r_b)
     gr = dv * (_at(lam, comps.r_a) - _at(lam, comps.r_b)) / comps.r_ohms ** 2
     gc = np.zeros(len(comps.c_farads))
@@ -62,11 +79,22 @@ def backstamp(sysm, comps, x, xprev, lam, h):
     return gr, gc, gd
 
 
+def backstamp_mosfets(sysm, x, lam):
+    """-lambda^T dF/d|VTO| and -lambda^T dF/dKP per MOSFET: the drain current
+    enters F at the drain row and leaves at the source row."""
+    if not len(sysm.mosfet_descriptors):
+        return np.zeros(0), np.zeros(0)
+    dr, so, di_dvto, di_dkp = _mosfet_terms(sysm, x)
+    dl = _at(lam, dr) - _at(lam, so)
+    return -dl * di_dvto, -dl * di_dkp
+
+
 def dc_adjoint(sysm, comps, x, w):
     J = _jacobian(sysm, sysm.g.val, x)
     lam = spl.splu(J.T.tocsc()).solve(np.asarray(w, dtype=np.float64))
     gr, _, gd = backstamp(sysm, comps, x, None, lam, 1.0)
-    return {"R": gr, "Is": gd}, lam
+    gv, gk = backstamp_mosfets(sysm, x, lam)
+    return {"R": gr, "Is": gd, "VTO": gv, "KP": gk}, lam
 
 
 def transient_states(sysm, x0, t0, h, n_steps):
@@ -90,19 +118,25 @@ def transient_adjoint(sysm, comps, states, h, w):
     gr = np.zeros(len(comps.r_ohms))
     gc = np.zeros(len(comps.c_farads))
     gd = np.zeros(len(sysm.diode_descriptors))
+    gv = np.zeros(len(sysm.mosfet_descriptors))
+    gk = np.zeros(len(sysm.mosfet_descriptors))
     N = len(states) - 1
     for k in range(N, 0, -1):
         J = _jacobian(sysm, A, states[k])
         lam = spl.splu(J.T.tocsc()).solve(rhs)
         a, b, c = backstamp(sysm, comps, states[k], states[k - 1], lam, h)
+        mv, mk = backstamp_mosfets(sysm, states[k], lam)
         gr += a
         gc += b
         gd += c
+        gv += mv
+        gk += mk
         rhs = cm.T @ lam / h
     J0 = _jacobian(sysm, sysm.g.val, states[0])
     lam0 = spl.splu(J0.T.tocsc()).solve(rhs)
     a, _, c = backstamp(sysm, comps, states[0], None, lam0, h)
-    return {"R": gr + a, "C": gc, "Is": gd + c}
+    mv, mk = backstamp_mosfets(sysm, states[0], lam0)
+    return {"R": gr + a, "C": gc, "Is": gd + c, "VTO": gv + mv, "KP": gk + mk}
 
 
 def _dF_dp(sysm, comps, kind, j, x, xprev, h):
@@ -126,6 +160,11 @@ def _dF_dp(sysm, comps, kind, j, x, xprev, h):
         ddv = (v(x, a) - v(x, b)) - (v(xprev, a) - v(xprev, b))
         put(a, ddv / h)
         put(b, -ddv / h)
+    elif kind in ("VTO", "KP"):
+        dr, so, di_dvto, di_dkp = _mosfet_terms(sysm, x)
+        d = di_dvto[j] if kind == "VTO" else di_dkp[j]
+        put(int(dr[j]), d)
+        put(int(so[j]), -d)
     else:
         an, ca, em1 = _diode_terms(sysm, x)
         put(int(an[j]), em1[j])

@@ -11,8 +11,10 @@ J x = b_eq directly; limit; converged when max|x - x_old| < abs_tol.
 The oracle's own default tolerance is tight (abs_tol 1e-13 relative to
 max(1, |x|_inf)) so that its answer is the FP64 fixed point.
 
-Continuation fallbacks (GMIN stepping, src/analysis/dc.rs:160-292) are used
-when the direct Newton does not converge.
+Continuation fallbacks: ``dc_operating_point`` adds GMIN stepping
+(src/analysis/dc.rs:160-292) when the direct Newton does not converge;
+``run_nonlinear`` restates the reference's whole DC strategy (source
+stepping, GMIN stepping, pseudo-transient continuation, dc.rs:60-650).
 """
 from __future__ import annotations
 
@@ -79,6 +81,111 @@ def dc_operating_point(sysm, **kw):
                 raise
             gmin = last_good * 10.0 ** (-sub)
     return newton(sysm, x0=x_prev, **kw)
+
+
+def _node_diagonals(sysm):
+    return np.array([sysm.g.value_index(i, i) for i in range(sysm.n_nodes)], dtype=np.int64)
+
+
+def _step(sysm, diag, gmin=0.0, base_b=None, x0=None, max_iterations=50, abs_tol=1e-9):
+    """``gmin_newton_step`` (dc.rs:293-330): one Newton solve with ``gmin``
+    added to every node diagonal and the given rhs; every linear solve is the
+    LU (the reference's CpuSparseLu retry of each step)."""
+    vals = sysm.g.val.copy()
+    if gmin != 0.0:
+        vals[diag] += gmin
+    x, _ = newton(sysm, base_vals=vals, base_b=base_b, x0=x0, max_iterations=max_iterations, abs_tol=abs_tol)
+    return x
+
+
+def run_nonlinear(sysm, step_tol=1e-9, stages=None):
+    """The reference's nonlinear DC strategy, ``run_nonlinear``
+    (src/analysis/dc.rs:60-290), with an LU per Newton iteration:
+
+      1. direct Newton (50 iterations, NewtonParams::default, :72-121);
+      2. for circuits with MOSFETs, source stepping (:495-645): alpha from
+         0.1, on success grow by twice the last successful step, on failure
+         halve towards the last good alpha, at most 20 subdivisions or a step
+         below 1e-6; 30 Newton iterations per step;
+      3. adaptive GMIN stepping (:160-253) from zeros: 1e-1, 1000x drops,
+         10x subdivisions from the last good level, at most 13; 15 Newton
+         iterations per step; then the true-GMIN solve (50 iterations);
+      4. if that fails, pseudo-transient continuation (:331-490) from the
+         last GMIN point: alpha from 1e-1, 100x drops, at most 7 10x
+         subdivisions, gmin = alpha and b += alpha x_prev on node rows,
+         20 Newton iterations per step; final solve with 25 iterations.
+
+    Intermediate steps stop at max|dx| < ``step_tol``; the answer is then
+    polished by the oracle's tight Newton.  ``stages`` (a list) receives the
+    names of the stages that ran.  Returns x.
+    """
+    stages = [] if stages is None else stages
+    n_nodes = sysm.n_nodes
+    polish = lambda x: newton(sysm, x0=x, max_iterations=100)[0]   # noqa: E731
+    stages.append("direct")
+    try:
+        return polish(newton(sysm, max_iterations=50, abs_tol=step_tol)[0])
+    except (NewtonNotConverged, SolveError):
+        pass
+    diag = _node_diagonals(sysm)
+    if len(sysm.mosfet_descriptors):
+        stages.append("source")
+        x_prev = None
+        last, target, sub = 0.0, 0.1, 0
+        try:
+            while target <= 1.0:
+                try:
+                    x = _step(sysm, diag, 0.0, target * sysm.b_dc, x_prev, 30, step_tol)
+                except (NewtonNotConverged, SolveError):
+                    sub += 1
+                    if sub > 20:
+                        raise
+                    target = last + (target - last) / 2.0
+                    if target - last < 1e-6:
+                        raise
+                    continue
+                x_prev = x
+                prev_step = target - last
+                last = target
+                sub = 0
+                if abs(target - 1.0) < 1e-12:
+                    return polish(x)
+                target = min(target + 2.0 * prev_step, 1.0)
+        except (NewtonNotConverged, SolveError):
+            pass
+    stages.append("gmin")
+    x_prev = None
+    last, target, sub = 1.0, 1e-1, 0
+    while target > 1e-13:
+        try:
+            x_prev = _step(sysm, diag, target, None, x_prev, 15, step_tol)
+            last, sub = target, 0
+            target *= 1e-3
+        except (NewtonNotConverged, SolveError):
+            sub += 1
+            if sub > 13:
+                raise
+            target = last * 10.0 ** (-sub)
+    try:
+        return polish(_step(sysm, diag, 0.0, None, x_prev, 50, step_tol))
+    except (NewtonNotConverged, SolveError):
+        if x_prev is None:
+            raise
+    stages.append("pseudo")
+    last, target, sub = 1.0, 1e-1, 0
+    while target > 1e-8:
+        b = sysm.b_dc.copy()
+        b[:n_nodes] += target * x_prev[:n_nodes]
+        try:
+            x_prev = _step(sysm, diag, target, b, x_prev, 20, step_tol)
+            last, sub = target, 0
+            target *= 1e-2
+        except (NewtonNotConverged, SolveError):
+            sub += 1
+            if sub > 7:
+                raise
+            target = last * 10.0 ** (-sub)
+    return polish(_step(sysm, diag, 0.0, None, x_prev, 25, step_tol))
 
 
 def residual(sysm, x, base_vals=None, base_b=None):

@@ -200,3 +200,103 @@ def test_torch_autograd_wrapper():
         rm[j] *= 1 - 1e-6
         fd = 3.0 * (oracle_output(rp, cv) - oracle_output(rm, cv)) / (2e-6 * rv[j])
         assert abs(float(r.grad[j]) - fd) <= 1e-6 * max(abs(fd), 1e-3 * float(r.grad.abs().max())), (j, fd)
+
+
+# ---- MOSFET |VTO| and KP (descriptor values; KP carries W/L) ----
+
+def _chain_case(stages, vin):
+    from tests.test_oracle_adjoint import analog_chain
+    ckt = analog_chain(stages=stages, vin=vin)
+    s = mna.compile_circuit(ckt)
+    return ckt, s, S.ComponentTable(ckt, s)
+
+
+def test_dc_adjoint_mosfet_gradients():
+    """Inverter chain with its first stage on its transfer curve (input
+    0.82 V): the GPU's d V(out_1) / d(|VTO|, KP) of every MOSFET against the
+    oracle's LU adjoint
+    and forward sensitivities (1e-8) and against central differences of the
+    oracle's Newton on the f32 descriptor values (1e-6)."""
+    import torch
+    from tests.test_oracle_adjoint import _fd
+    ckt, s, comps = _chain_case(4, 0.82)
+    x, _ = newton_ref.newton(s)
+    probe = s.node_index(2 + 1)
+    w = np.zeros(s.size)
+    w[probe] = 1.0
+    ref, _ = adjoint_ref.dc_adjoint(s, comps, x, w)
+    plan = S.NewtonPlan(s)
+    try:
+        xd = torch.from_numpy(x).cuda()
+        g, _, _ = S.adjoint_dc(plan, xd.data_ptr(), w, comps, _krylov())
+    finally:
+        plan.close()
+    for kind in ("VTO", "KP"):
+        scale = np.max(np.abs(ref[kind]))
+        assert scale > 0.0
+        assert np.max(np.abs(g[kind] - ref[kind])) <= 1e-8 * scale, kind
+        for j in range(len(s.mosfet_descriptors)):
+            fs = adjoint_ref.forward_sensitivity(s, comps, [x], 1.0, w, kind, j)
+            assert abs(g[kind][j] - fs) <= 1e-8 * max(abs(fs), scale), (kind, j)
+        for j in (0, 1):
+            fd = _fd(s, kind, j, lambda s2: newton_ref.newton(s2, x0=x)[0][probe])
+            assert abs(g[kind][j] - fd) <= 1e-6 * max(abs(fd), 1e-3 * scale), (kind, j, g[kind][j], fd)
+
+
+def test_transient_adjoint_mosfet_gradients():
+    """Backward Euler through the input's rising edge (12 steps of 5 ps,
+    checkpoints every 5): d V(out_1) / d(|VTO|, KP) against the oracle's LU
+    adjoint and forward sensitivities (1e-8); the gradient flows through a
+    torch.autograd.Function over the C ABI."""
+    import torch
+    hh = 5e-12
+    ckt, s, comps = _chain_case(3, 0.0)
+    x0, _ = newton_ref.dc_operating_point(s)
+    probe = s.node_index(2 + 1)
+    w = np.zeros(s.size)
+    w[probe] = 1.0
+    n_steps = 12
+    states = adjoint_ref.transient_states(s, x0, 0.0, hh, n_steps)
+    ref = adjoint_ref.transient_adjoint(s, comps, states, hh, w)
+
+    def gpu(sysm):
+        plan = S.NewtonPlan(sysm)
+        tr = S.Transient(plan, [])
+        try:
+            xd = torch.from_numpy(x0).cuda()
+            return tr.adjoint(xd.data_ptr(), 0.0, hh, n_steps, w, comps, _newton(), 5, _krylov())
+        finally:
+            tr.close()
+            plan.close()
+
+    g, info = gpu(s)
+    assert info["output"] == pytest.approx(states[-1][probe], rel=1e-10)
+    for kind in ("VTO", "KP"):
+        scale = np.max(np.abs(ref[kind]))
+        assert scale > 0.0
+        assert np.max(np.abs(g[kind] - ref[kind])) <= 1e-8 * scale, kind
+        for j in (0, 1, 4):
+            fs = adjoint_ref.forward_sensitivity(s, comps, states, hh, w, kind, j)
+            assert abs(g[kind][j] - fs) <= 1e-8 * max(abs(fs), scale), (kind, j)
+
+    class ChainOutput(torch.autograd.Function):
+        """o(|VTO|, KP) of the transient, gradient from the adjoint entry point."""
+        @staticmethod
+        def forward(ctx, vto, kp):
+            s2 = copy.deepcopy(s)
+            s2.mosfet_descriptors["vto"] = vto.detach().numpy().astype(np.float32)
+            s2.mosfet_descriptors["kp"] = kp.detach().numpy().astype(np.float32)
+            g2, info2 = gpu(s2)
+            ctx.save_for_backward(torch.from_numpy(g2["VTO"]), torch.from_numpy(g2["KP"]))
+            return torch.tensor(info2["output"], dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            gv, gk = ctx.saved_tensors
+            return grad_out * gv, grad_out * gk
+
+    vto = torch.tensor(s.mosfet_descriptors["vto"].astype(np.float64), requires_grad=True)
+    kp = torch.tensor(s.mosfet_descriptors["kp"].astype(np.float64), requires_grad=True)
+    (2.0 * ChainOutput.apply(vto, kp)).backward()
+    np.testing.assert_allclose(vto.grad.numpy(), 2.0 * g["VTO"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(kp.grad.numpy(), 2.0 * g["KP"], rtol=1e-12, atol=0)

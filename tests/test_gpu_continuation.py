@@ -52,6 +52,26 @@ def test_gmin_stepping_recovers_capped_direct_solve(ctx):
     assert _rel(x[s.n_nodes:], ref[s.n_nodes:]) < 1e-9
 
 
+def test_pseudo_transient_stage_runs_and_converges(ctx):
+    """Pseudo-transient continuation (dc.rs:331-490) after GMIN stepping: the
+    testing flag makes the true-GMIN solve count as failed, so the stage runs
+    from the last GMIN point (alpha from 0.1, 100x drops, b += alpha x_good on
+    node rows) and its final 25-iteration true-DC solve reaches the oracle's
+    operating point."""
+    s = mna.compile_circuit(ck.diode_mesh(10, 10, seed=2))
+    ref, _ = newton_ref.newton(s)
+    x, info = _plan_solve(ctx, s, _params(3, continuation=S._lib.CONT_ON | S._lib.CONT_TEST_PSEUDO))
+    assert info["continuation_kind"] == CONT_PSEUDO
+    # GMIN levels 0.1 .. 1e-13 (5), the true-GMIN solve, alpha 0.1 .. 1e-7 (4), the final solve
+    assert info["continuation_steps"] >= 11
+    assert _rel(x[: s.n_nodes], ref[: s.n_nodes]) < 1e-9
+    assert _rel(x[s.n_nodes:], ref[s.n_nodes:]) < 1e-9
+    # without the flag the same call ends after GMIN stepping
+    x2, info2 = _plan_solve(ctx, s, _params(3))
+    assert info2["continuation_kind"] == CONT_GMIN
+    assert info2["continuation_steps"] < info["continuation_steps"]
+
+
 def test_source_stepping_for_mosfet_circuit(ctx):
     """Circuits with MOSFETs try source stepping first (dc.rs:133-152); its
     last step (all sources at full value) is the true DC solve."""

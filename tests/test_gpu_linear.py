@@ -175,6 +175,13 @@ def test_backend_ops(ctx):
                                rtol=1e-13, atol=1e-13)
     by.upload(y0)
     assert abs(be.dot(bx, by) - float(x @ y0)) < 1e-12 * abs(x).sum() * abs(y0).max()
+    # dot_n (backend.rs:60-68): owned entries only
+    k = s.size // 3
+    assert abs(be.dot_n(bx, by, k) - float(x[:k] @ y0[:k])) < 1e-12 * abs(x[:k]).sum() * abs(y0).max()
+    assert be.dot_n(bx, by, 0) == 0.0
+    assert be.dot_n(bx, by, s.size) == be.dot(bx, by)
+    with pytest.raises(S.InvalidArgument):
+        be.dot_n(bx, by, s.size + 1)
     be.axpy(2.5, bx, by)
     np.testing.assert_allclose(by.download(), y0 + 2.5 * x, rtol=0, atol=1e-15)
     be.scale(-3.0, by)
