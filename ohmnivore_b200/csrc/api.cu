@@ -158,6 +158,28 @@ static int choose_lpr(int64_t n, int64_t nnz) {
 
 static constexpr int kBlock = kSolverBlock;
 
+// Dynamic shared memory for the Krylov slice of a block that owns `rows`
+// rows: records, r_hat, t, d, weights (FP64, the larger of the two Krylov
+// precisions), row pointers and pair flags per row, column + value per
+// nonzero outside long rows (an estimate with a 3 % margin; a block whose
+// slice is larger works from global memory), or 0 when it cannot fit.
+int ohm_krylov_smem_bytes(KernelFn fn, int64_t n, int64_t nnz_short, int grid) {
+    if (n <= 0 || grid <= 0) return 0;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, (const void *)fn) != cudaSuccess) return 0;
+    const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024;
+    const int64_t rows = (n + grid - 1) / grid + 1;
+    const int64_t nnz_blk = (int64_t)((double)std::max<int64_t>(nnz_short, 0) * (double)rows / (double)n * 1.03) + 256;
+    const int64_t need = rows * (32 + 8 + 8 + 8 + 8 + 4 + 1) + nnz_blk * (8 + 4) + 16 * 16;
+    if (need > avail) return 0;
+    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess)
+        return 0;
+    return (int)need;
+}
+
 ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t nnz, int *launches) {
     const int lpr = choose_lpr(a.n, nnz);
     KernelFn fn = pick_kernel(lpr);
@@ -171,13 +193,22 @@ ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t n
     int64_t cap = (int64_t)per_sm * t.num_sms;
     if (t.max_grid > 0) cap = std::min<int64_t>(cap, t.max_grid);
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+    // one block per SM either way: a block is 1024 threads at the register cap
+    a.smem_bytes = ohm_krylov_smem_bytes(fn, a.n, nnz - a.nnz_long, grid);
+    if (a.smem_bytes > 0) {
+        int fit = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kBlock, a.smem_bytes));
+        if (fit < 1) a.smem_bytes = 0;
+        else grid = std::min<int64_t>(grid, (int64_t)fit * t.num_sms);
+    }
     a.gs.count = (unsigned long long *)t.sync_words;     // words 0-1
     a.gs.error = (int *)(t.sync_words + 2);              // word 2
     a.info = t.info_dev;
     CUDA_TRY(cudaMemsetAsync(t.sync_words, 0, 4 * sizeof(unsigned int), t.stream));
     CUDA_TRY(cudaMemsetAsync(t.info_dev, 0, sizeof(DeviceInfo), t.stream));
     void *args[] = {&a};
-    CUDA_TRY(cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kBlock), args, 0, t.stream));
+    CUDA_TRY(cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kBlock), args, (size_t)a.smem_bytes,
+                                         t.stream));
     if (launches) *launches += 1;
     return OHM_OK;
 }
@@ -497,6 +528,7 @@ struct ohm_plan {
     uint8_t *stampflag = nullptr;      // per row: diagonal / rhs written by the stamp map
     // long rows and long stamp segments (team-cooperative)
     int n_long = 0, n_long_chunks = 0, n_lseg = 0, n_lseg_chunks = 0;
+    int64_t nnz_long = 0;              // nonzeros in long rows
     uint8_t *longflag = nullptr, *lseg_flag = nullptr;
     uint32_t *long_row = nullptr, *long_chunk_ptr = nullptr, *long_chunk_owner = nullptr, *long_chunk_beg = nullptr,
              *long_chunk_end = nullptr;
@@ -590,6 +622,7 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     split_long((int64_t)rs.size(), rptr.data(), kLongSegMin, kLongSegChunk, (int64_t)ms.size(), lsegs);
     p->n_long = (int)lrows.item.size();
     p->n_long_chunks = (int)lrows.chunk_beg.size();
+    for (uint32_t r : lrows.item) p->nnz_long += row_ptrs[r + 1] - row_ptrs[r];
     p->n_lseg = (int)lsegs.item.size();
     p->n_lseg_chunks = (int)lsegs.chunk_beg.size();
     p->h_rp.assign(row_ptrs, row_ptrs + size + 1);
@@ -746,7 +779,7 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.n_nodes = (int)std::min<int64_t>(np->n_nodes, p->n);
     a.stampflag = p->stampflag;
     a.x_good = p->x_good;
-    a.n_long = p->n_long; a.n_long_chunks = p->n_long_chunks; a.longflag = p->longflag;
+    a.n_long = p->n_long; a.n_long_chunks = p->n_long_chunks; a.longflag = p->longflag; a.nnz_long = p->nnz_long;
     a.long_row = p->long_row; a.long_chunk_ptr = p->long_chunk_ptr; a.long_chunk_owner = p->long_chunk_owner;
     a.long_chunk_beg = p->long_chunk_beg; a.long_chunk_end = p->long_chunk_end; a.long_part = p->long_part;
     a.n_lseg = p->n_lseg; a.n_lseg_chunks = p->n_lseg_chunks; a.lseg_flag = p->lseg_flag; a.lseg = p->lseg;

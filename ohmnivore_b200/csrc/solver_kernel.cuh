@@ -180,6 +180,11 @@ struct KernelArgs {
     double *partials;           // >= 8 * gridDim.x doubles (two alternating regions)
     GridSync gs;
     DeviceInfo *info;
+    // dynamic shared memory of the launch (grid-team kernels): when > 0 the
+    // Krylov solve keeps each block's slice there if it fits (krylov()).
+    // nnz_long: nonzeros of the long rows (host side, sizes that slice).
+    int smem_bytes;
+    int64_t nnz_long;
 };
 
 // Columns of the per-outer-iteration trace: FP32 Krylov iterations, FP64
@@ -241,15 +246,16 @@ __device__ __forceinline__ T cvt(double x) { return (T)x; }
 // and gathers are issued together), so the dependent L2 round trips of one row
 // overlap those of the others.  All lanes of a warp run the same number of
 // tiles and inner steps, so the group shuffles are safe.  `slow` is the row's
-// flag from `rowflag` (false when null).
+// flag from `rowflag` (false when null).  rp is indexed by row - rp_off (a
+// block's local CSR slice has rp_off = its first row).
 constexpr int kRowsInFlight = 4;
 
-template <int LPR, typename Acc, typename TA, typename X, typename F>
+template <int LPR, typename Acc, typename TA, typename X, typename F, int U = kRowsInFlight>
 __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
                                           const uint32_t *__restrict__ col,
                                           const TA *__restrict__ val, const uint8_t *rowflag,
-                                          int r0, int r1, X x, F f, const uint8_t *skip = nullptr) {
-    constexpr int U = kRowsInFlight;
+                                          int r0, int r1, X x, F f, const uint8_t *skip = nullptr,
+                                          int rp_off = 0) {
     const int lane = threadIdx.x % LPR;
     const int group = threadIdx.x / LPR;
     const int ngroups = blockDim.x / LPR;
@@ -263,8 +269,8 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
         for (int u = 0; u < U; ++u) {
             row[u] = tile + group + u * ngroups;
             const bool ok = row[u] < r1 && !(skip != nullptr && skip[row[u]] != 0);
-            beg[u] = ok ? rp[row[u]] : 0u;
-            end[u] = ok ? rp[row[u] + 1] : 0u;
+            beg[u] = ok ? rp[row[u] - rp_off] : 0u;
+            end[u] = ok ? rp[row[u] - rp_off + 1] : 0u;
             slow[u] = ok && rowflag != nullptr && rowflag[row[u]] != 0;
             acc[u] = Acc(0);
         }
@@ -296,10 +302,13 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
 // connected device) are skipped by spmv_rows and computed by the whole team:
 // one warp per chunk of at most a few hundred nonzeros writes a partial, a
 // team sync, then one warp per long row sums its partials in a fixed order
-// and calls f(row, y) like spmv_rows does.  Returns false if the sync gave up.
+// and calls f(row, y) like spmv_rows does.  With own_only, each long row is
+// finished by the block that owns it (the callback then may use that block's
+// shared memory).  Returns false if the sync gave up.
 template <typename Acc, class Team, typename TA, typename X, typename F>
 __device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const uint32_t *__restrict__ col,
-                                          const TA *__restrict__ val, const uint8_t *rowflag, X x, F f) {
+                                          const TA *__restrict__ val, const uint8_t *rowflag, X x, F f,
+                                          bool own_only = false) {
     if (a.n_long == 0) return true;
     const int lane = threadIdx.x & 31;
     const int warp = g.gtid >> 5, nwarps = g.gstride >> 5;
@@ -315,7 +324,10 @@ __device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const ui
         if (lane == 0) a.long_part[c] = s;
     }
     if (!g.sync()) return false;
-    for (int j = warp; j < a.n_long; j += nwarps) {
+    const int j0 = own_only ? (int)(threadIdx.x >> 5) : warp;
+    const int js = own_only ? (int)(blockDim.x >> 5) : nwarps;
+    for (int j = j0; j < a.n_long; j += js) {
+        if (own_only && ((int)a.long_row[j] < g.r0 || (int)a.long_row[j] >= g.r1)) continue;
         double s = 0.0;
         for (uint32_t c = a.long_chunk_ptr[j] + lane; c < a.long_chunk_ptr[j + 1]; c += 32) s += a.long_part[c];
 #pragma unroll
@@ -341,6 +353,42 @@ struct KrylovOut {
     int restarts;
 };
 
+// Dynamic shared memory of the grid-team kernels: the Krylov solve keeps
+// each block's own-row state and CSR slice here when the launch provides
+// enough of it (KernelArgs::smem_bytes).
+extern __shared__ __align__(128) unsigned char ohm_dsmem[];
+
+// Exclusive prefix sum over the block of one value per thread (in thread
+// order); *total receives the block sum.  `scratch` holds >= 33 words.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *scratch, uint32_t *total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    __syncthreads();
+    if (lane == 31) scratch[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nwarps ? scratch[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        scratch[lane] = w;                       // inclusive prefix of warp sums
+        if (lane == 31) scratch[32] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? scratch[warp - 1] : 0u) + inc - v;
+    *total = scratch[32];
+    __syncthreads();
+    return before;
+}
+
 // Right-preconditioned BiCGSTAB on J d = r64 in precision T, d0 = 0, with
 // the reference's operation order (bicgstab.rs:104-183) and three grid
 // synchronisations per iteration:
@@ -348,40 +396,52 @@ struct KrylovOut {
 //       gathered record), reduce (r_hat, v), (v, v)
 //   CD: s = r - a v and t = A M^-1 s (on the fly), reduce (s, s), (t, s), (t, t)
 //   E : d += a phat + w shat; r = s - w t, reduce (r_hat, r), (r, r)
-// The early exit on ||s|| (bicgstab.rs:134-139) is taken after CD; t is then
-// simply unused.  Stops when ||r|| < max(tol_floor, inner_rtol * ||r0||).  On
-// success the correction is left in a.dx (FP64) for the rows of this block.
+// phat = M^-1 p, s and shat = M^-1 s are re-formed from the row's record
+// where they are needed instead of being stored (the same expressions, so
+// the same values).  The early exit on ||s|| (bicgstab.rs:134-139) is taken
+// after CD; t is then simply unused.  Stops when ||r|| < max(tol_floor,
+// inner_rtol * ||r0||).  On success the correction is left in a.dx (FP64)
+// for the rows of this block.
+//
+// This is the global-memory form (batches, systems whose slices do not fit
+// in shared memory); krylov_smem() is the same iteration with each block's
+// slice in shared memory.
 //
 // Newton solves measure that stopping norm on the diagonally scaled residual
 // W r, w_i = 1/|J_ii| (1 for a zero diagonal): volts instead of amperes, so a
 // junction row with a huge conductance cannot hide unresolved corrections on
-// the other rows behind a relative tolerance.  a.dx holds w during the solve.
-// Linear solves keep the reference's unscaled ||r|| < tol ||b||.
+// the other rows behind a relative tolerance.  Linear solves keep the
+// reference's unscaled ||r|| < tol ||b||.
 template <typename T, int LPR, class Team>
 __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                       int max_it, bool accept_partial, KrylovOut &out) {
     using Acc = T;   // FP32 SpMV accumulates in FP32, FP64 in FP64; dots always in FP64
     const int r0 = g.r0, r1 = g.r1;
     KRec<T> *cur = (KRec<T> *)a.rec0, *nxt = (KRec<T> *)a.rec1;
-    T *rhat = (T *)a.rhat, *s = (T *)a.s, *t = (T *)a.t;
-    T *phat = (T *)a.phat, *shat = (T *)a.shat, *d = (T *)a.d, *pc_part = (T *)a.pc_part;
+    T *pc_part = (T *)a.pc_part;
     const int32_t *partner = a.partner;
     const T *A;
     if constexpr (sizeof(T) == 4) A = (const T *)a.vals32; else A = (const T *)a.vals64;
     out.iterations = 0;
     out.restarts = 0;
+    const bool wt = a.newton != 0;
+
+    T *rhat = (T *)a.rhat + r0, *t = (T *)a.t + r0, *d = (T *)a.d + r0;   // own rows, local index
+    T *s_pair = (T *)a.s;   // s of the rows of 2x2 pairs (read by the partner in E)
+    double *w = a.dx + r0;
+    auto own = [&](KRec<T> *buf, int i) -> KRec<T> { return buf[i]; };
+    auto is_paired = [&](int i) -> bool { return partner[i] >= 0; };
 
     // ---- start: r = r64, r_hat = r, p = v = d = 0; preconditioner coefficients ----
-    const bool wt = a.newton != 0;
-    double *w = a.dx;
     double acc0[2] = {0.0, 0.0};     // ||r||^2, ||W r||^2
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const int li = i - r0;
         const T rt = cvt<T>(a.r64[i]);
         double cs = 0.0, cp = 0.0;
         const uint32_t ds = a.diag_slot[i];
         const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
         const double wi = (wt && fabs(aii) > 1e-30) ? 1.0 / fabs(aii) : 1.0;
-        if (wt) w[i] = wi;
+        if (wt) w[li] = wi;
         if (a.precond != kPcNone) {
             const int pi = partner[i];
             if (a.precond == kPcAuto && pi >= 0) {
@@ -402,8 +462,8 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
         q.p = T(0); q.v = T(0); q.r = rt; q.c = cvt<T>(cs);
         cur[i] = q;
         pc_part[i] = cvt<T>(cp);
-        rhat[i] = rt;
-        d[i] = T(0);
+        rhat[li] = rt;
+        d[li] = T(0);
         acc0[0] += (double)rt * (double)rt;
         acc0[1] += (wi * (double)rt) * (wi * (double)rt);
     }
@@ -425,16 +485,25 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
 #define OHM_RESTART()                                                          \
     do {                                                                       \
         for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {              \
-            KRec<T> q = cur[i];                                                \
+            KRec<T> q = own(cur, i);                                           \
             q.p = T(0); q.v = T(0);                                            \
             cur[i] = q;                                                        \
-            rhat[i] = q.r;                                                     \
+            rhat[i - r0] = q.r;                                                \
         }                                                                      \
         OHM_SYNC_OR(kKrylovAbort);                                             \
         rho = 1.0; alpha = 1.0; omega = 1.0;                                   \
         rho_new = rr_cur; rhat2 = rr_cur;                                      \
         ++out.restarts;                                                        \
     } while (0)
+
+    // M^-1 applied to a row's own vector u (the self coefficient c of the
+    // row's record, plus the partner term for a 2x2 pair): the same
+    // expression as in the gathers below, so the same rounding.
+    auto pc_apply = [&](int i, double c, T u, bool pair, T u_partner) -> T {
+        double z = c * (double)u;
+        if (pair) z += (double)pc_part[i] * (double)u_partner;
+        return cvt<T>(z);
+    };
 
     if (!isfinite(r0norm)) {
         code = kKrylovNan;
@@ -468,16 +537,15 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             };
             double acc1[2] = {0.0, 0.0};
             auto ab_row = [&](int i, double y) {
-                const KRec<T> q = cur[i];
-                KRec<T> o;
-                o.p = pnew(q);
-                o.v = cvt<T>(y);
-                o.r = q.r;
-                o.c = q.c;
-                nxt[i] = o;
-                phat[i] = phat_at(i, true);
-                acc1[0] += (double)rhat[i] * (double)o.v;
-                acc1[1] += (double)o.v * (double)o.v;
+                const KRec<T> q = own(cur, i);
+                KRec<T> n;
+                n.p = pnew(q);
+                n.v = cvt<T>(y);
+                n.r = q.r;
+                n.c = q.c;
+                nxt[i] = n;
+                acc1[0] += (double)rhat[i - r0] * (double)n.v;
+                acc1[1] += (double)n.v * (double)n.v;
             };
             spmv_rows<LPR, Acc>(a.row_ptr, a.col, A, a.rowflag, r0, r1, phat_at, ab_row, a.longflag);
             if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row)) return kKrylovAbort;
@@ -494,6 +562,11 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             }
             alpha = rho / acc1[0];
             const double al = alpha;
+            // phat of an own row from its record in nxt (p is the new p)
+            auto phat_own = [&](int i, const KRec<T> &q) -> T {
+                const bool pair = is_paired(i);
+                return pc_apply(i, (double)q.c, q.p, pair, pair ? nxt[partner[i]].p : T(0));
+            };
             // ---------------- CD: s = r - a v and t = A M^-1 s ----------------
             auto s_of = [&](const KRec<T> &q) -> T {
                 return cvt<T>((double)q.r + (-al) * (double)q.v);
@@ -509,12 +582,11 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             };
             double acc3[4] = {0.0, 0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t), ||W s||^2
             auto cd_row = [&](int i, double y) {
-                const T si = s_of(nxt[i]);
+                const T si = s_of(own(nxt, i));
                 const T ti = cvt<T>(y);
-                s[i] = si;
-                t[i] = ti;
-                shat[i] = shat_at(i, true);
-                const double ws = wt ? w[i] * (double)si : (double)si;
+                t[i - r0] = ti;
+                if (is_paired(i)) s_pair[i] = si;
+                const double ws = wt ? w[i - r0] * (double)si : (double)si;
                 acc3[0] += (double)si * (double)si;
                 acc3[1] += (double)ti * (double)si;
                 acc3[2] += (double)ti * (double)ti;
@@ -526,8 +598,10 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
                 if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
             }
             if (sqrt(acc3[3]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
-                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-                    d[i] = cvt<T>((double)d[i] + al * (double)phat[i]);
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                    const T ph = phat_own(i, own(nxt, i));
+                    d[i - r0] = cvt<T>((double)d[i - r0] + al * (double)ph);
+                }
                 code = kKrylovConverged;
                 ++it;
                 break;
@@ -537,11 +611,19 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
             // ---------------- E: d, r updates ----------------
             double acc4[3] = {0.0, 0.0, 0.0};   // (r_hat, r), ||r||^2, ||W r||^2
             for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                d[i] = cvt<T>(((double)d[i] + al * (double)phat[i]) + omega * (double)shat[i]);
-                const T rt = cvt<T>((double)s[i] + (-omega) * (double)t[i]);
+                const int li = i - r0;
+                const KRec<T> q = own(nxt, i);
+                const bool pair = is_paired(i);
+                const int pi = pair ? partner[i] : i;
+                // the partner's p and s as formed in AB / CD (its r changes in this loop)
+                const T ph = pc_apply(i, (double)q.c, q.p, pair, pair ? nxt[pi].p : T(0));
+                const T si = s_of(q);
+                const T sh = pc_apply(i, (double)q.c, si, pair, pair ? s_pair[pi] : T(0));
+                d[li] = cvt<T>(((double)d[li] + al * (double)ph) + omega * (double)sh);
+                const T rt = cvt<T>((double)si + (-omega) * (double)t[li]);
                 nxt[i].r = rt;
-                const double wr = wt ? w[i] * (double)rt : (double)rt;
-                acc4[0] += (double)rhat[i] * (double)rt;
+                const double wr = wt ? w[li] * (double)rt : (double)rt;
+                acc4[0] += (double)rhat[li] * (double)rt;
                 acc4[1] += (double)rt * (double)rt;
                 acc4[2] += wr * wr;
             }
@@ -566,7 +648,7 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
 #undef OHM_RESTART
     out.iterations = it;
     if (code == kKrylovConverged)
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.dx[i] = (double)d[i];
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.dx[i] = (double)d[i - r0];
     return code;
 }
 
@@ -576,11 +658,298 @@ __device__ __forceinline__ int krylov(const KernelArgs &a, Team &g, double tol_f
 
 namespace ohm {
 
+// The slice of krylov_smem() does not fit in the launch's shared memory.
+constexpr int kKrylovNoSmem = -2;
+
+// krylov() with each block's slice in shared memory: the CSR rows it owns
+// (local row pointers, columns, values in the Krylov precision; long rows
+// stay with the team), its rows' records, r_hat, t, d, the Newton weights
+// and a pair flag.  Every phase then reads global memory only for the
+// neighbours' records that the SpMV gathers, and the own-row updates touch
+// shared memory (addressed with 32-bit offsets) plus the published record
+// fields.  The arithmetic and its order are krylov()'s, so the results are
+// the same.  The slice is laid out per solve (the values change with every
+// Newton iteration); a block whose slice does not fit returns kKrylovNoSmem
+// before touching anything, and the caller runs krylov() (a per-block
+// choice: blocks exchange data only through the global records and the
+// reductions).  U rows per group are in flight in each SpMV tile.
+template <typename T, int LPR, int U>
+__device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, double tol_floor, double inner_rtol,
+                                           int max_it, bool accept_partial, KrylovOut &out) {
+    using Acc = T;
+    const int r0 = g.r0, r1 = g.r1, R = r1 - r0;
+    if (a.smem_bytes == 0 || R <= 0) return kKrylovNoSmem;
+    const T *A;
+    if constexpr (sizeof(T) == 4) A = (const T *)a.vals32; else A = (const T *)a.vals64;
+    const bool wt = a.newton != 0;
+    // ---- layout: local row pointers by a block scan over contiguous chunks ----
+    const int chunk = (R + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int c0 = min(R, (int)threadIdx.x * chunk), c1 = min(R, c0 + chunk);
+    uint32_t mine = 0;
+    for (int li = c0; li < c1; ++li) {
+        const int i = r0 + li;
+        if (!(a.longflag != nullptr && a.longflag[i] != 0)) mine += a.row_ptr[i + 1] - a.row_ptr[i];
+    }
+    uint32_t nloc = 0;
+    const uint32_t before = block_exclusive_scan(mine, (uint32_t *)g.smem, &nloc);
+    auto up16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+    const uint32_t o_rhat = up16((uint32_t)R * (uint32_t)sizeof(KRec<T>));
+    const uint32_t o_t = o_rhat + up16((uint32_t)R * (uint32_t)sizeof(T));
+    const uint32_t o_d = o_t + up16((uint32_t)R * (uint32_t)sizeof(T));
+    const uint32_t o_w = o_d + up16((uint32_t)R * (uint32_t)sizeof(T));
+    const uint32_t o_val = o_w + (wt ? up16((uint32_t)R * 8u) : 0u);
+    const uint32_t o_col = o_val + up16(nloc * (uint32_t)sizeof(T));
+    const uint32_t o_rp = o_col + up16(nloc * 4u);
+    const uint32_t o_pair = o_rp + up16((uint32_t)(R + 1) * 4u);
+    const uint32_t o_end = o_pair + up16((uint32_t)R);
+    if (o_end > (uint32_t)a.smem_bytes) return kKrylovNoSmem;      // uniform over the block
+    KRec<T> *rec = (KRec<T> *)ohm_dsmem;
+    T *rhat = (T *)(ohm_dsmem + o_rhat);
+    T *t = (T *)(ohm_dsmem + o_t);
+    T *d = (T *)(ohm_dsmem + o_d);
+    double *w = (double *)(ohm_dsmem + o_w);
+    T *lval = (T *)(ohm_dsmem + o_val);
+    uint32_t *lcol = (uint32_t *)(ohm_dsmem + o_col);
+    uint32_t *lrp = (uint32_t *)(ohm_dsmem + o_rp);
+    uint8_t *pair = ohm_dsmem + o_pair;
+    {
+        uint32_t pos = before;
+        for (int li = c0; li < c1; ++li) {
+            const int i = r0 + li;
+            lrp[li] = pos;
+            if (!(a.longflag != nullptr && a.longflag[i] != 0)) {
+                for (uint32_t k = a.row_ptr[i]; k < a.row_ptr[i + 1]; ++k, ++pos) {
+                    lcol[pos] = a.col[k];
+                    lval[pos] = A[k];
+                }
+            }
+        }
+        if (threadIdx.x == 0) lrp[R] = nloc;
+    }
+    out.iterations = 0;
+    out.restarts = 0;
+    KRec<T> *cur = (KRec<T> *)a.rec0, *nxt = (KRec<T> *)a.rec1;
+
+    // ---- start: r = r64, r_hat = r, p = v = d = 0; preconditioner coefficients ----
+    double acc0[2] = {0.0, 0.0};     // ||r||^2, ||W r||^2
+    for (int li = threadIdx.x; li < R; li += blockDim.x) {
+        const int i = r0 + li;
+        const T rt = cvt<T>(a.r64[i]);
+        double cs = 0.0, cp = 0.0;
+        const uint32_t ds = a.diag_slot[i];
+        const double aii = ds == kSentinel ? 0.0 : a.vals64[ds];
+        const double wi = (wt && fabs(aii) > 1e-30) ? 1.0 / fabs(aii) : 1.0;
+        if (wt) w[li] = wi;
+        const int pi = a.partner[i];
+        if (a.precond != kPcNone) {
+            if (a.precond == kPcAuto && pi >= 0) {
+                const double akk = a.diag_slot[pi] == kSentinel ? 0.0 : a.vals64[a.diag_slot[pi]];
+                const double aik = a.vals64[a.off_slot[i]];
+                const double aki = a.vals64[a.off_slot[pi]];
+                const double det = aii * akk - aik * aki;
+                if (fabs(det) > 1e-300) { cs = akk / det; cp = -aik / det; }
+            } else if (fabs(aii) > 1e-30) {
+                cs = 1.0 / aii;
+            } else if (a.precond == kPcAuto) {
+                cs = 1.0;   // unpaired zero diagonal: identity keeps M^-1 nonsingular
+            }
+        } else {
+            cs = 1.0;
+        }
+        pair[li] = pi >= 0 ? 1 : 0;
+        KRec<T> q;
+        q.p = T(0); q.v = T(0); q.r = rt; q.c = cvt<T>(cs);
+        cur[i] = q;
+        rec[li] = q;
+        ((T *)a.pc_part)[i] = cvt<T>(cp);
+        rhat[li] = rt;
+        d[li] = T(0);
+        acc0[0] += (double)rt * (double)rt;
+        acc0[1] += (wi * (double)rt) * (wi * (double)rt);
+    }
+    if (!g.template allreduce<2>(acc0)) return kKrylovAbort;   // also orders the slice writes
+    const double r0norm = sqrt(acc0[1]);
+    const double abs_tol = fmax(tol_floor, inner_rtol * r0norm);
+    double rr_cur = acc0[0], rhat2 = acc0[0], rho_new = acc0[0];
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    int code = kKrylovRunning;
+    int it = 0;
+
+#define OHM_RESTART_S()                                                        \
+    do {                                                                       \
+        for (int li = threadIdx.x; li < R; li += blockDim.x) {                 \
+            KRec<T> q = rec[li];                                               \
+            q.p = T(0); q.v = T(0);                                            \
+            cur[r0 + li] = q;                                                  \
+            rec[li] = q;                                                       \
+            rhat[li] = q.r;                                                    \
+        }                                                                      \
+        OHM_SYNC_OR(kKrylovAbort);                                             \
+        rho = 1.0; alpha = 1.0; omega = 1.0;                                   \
+        rho_new = rr_cur; rhat2 = rr_cur;                                      \
+        ++out.restarts;                                                        \
+    } while (0)
+
+    auto pc_apply = [&](int i, double c, T u, bool pr, T u_partner) -> T {
+        double z = c * (double)u;
+        if (pr) z += (double)((const T *)a.pc_part)[i] * (double)u_partner;
+        return cvt<T>(z);
+    };
+
+    if (!isfinite(r0norm)) {
+        code = kKrylovNan;
+    } else if (r0norm < abs_tol || r0norm == 0.0) {
+        code = kKrylovConverged;
+    } else {
+        for (; it < max_it; ++it) {
+            if (!(fabs(rho_new) >= kBreakdownRel * sqrt(rhat2 * rr_cur))) {
+                if (out.restarts < a.max_restarts && rr_cur > 0.0) {
+                    OHM_RESTART_S();
+                } else {
+                    code = kKrylovBreakRho;
+                    break;
+                }
+            }
+            const double beta = (rho_new / rho) * (alpha / omega);
+            rho = rho_new;
+            const double om = omega;
+            // ---------------- AB: p update and v = A M^-1 p ----------------
+            auto pnew = [&](const KRec<T> &q) -> T {
+                return cvt<T>(((double)q.p + (-om) * (double)q.v) * beta + (double)q.r);
+            };
+            auto phat_at = [&](int j, bool slow) -> T {
+                const KRec<T> q = cur[j];
+                double z = (double)q.c * (double)pnew(q);
+                if (slow) {
+                    const int pj = a.partner[j];
+                    if (pj >= 0) z += (double)((const T *)a.pc_part)[j] * (double)pnew(cur[pj]);
+                }
+                return cvt<T>(z);
+            };
+            double acc1[2] = {0.0, 0.0};
+            auto ab_row = [&](int i, double y) {
+                const int li = i - r0;
+                const KRec<T> q = rec[li];
+                KRec<T> n;
+                n.p = pnew(q);
+                n.v = cvt<T>(y);
+                n.r = q.r;
+                n.c = q.c;
+                nxt[i] = n;
+                rec[li] = n;
+                acc1[0] += (double)rhat[li] * (double)n.v;
+                acc1[1] += (double)n.v * (double)n.v;
+            };
+            spmv_rows<LPR, Acc, T, decltype(phat_at), decltype(ab_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
+                                                                            phat_at, ab_row, a.longflag, r0);
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row, true)) return kKrylovAbort;
+            if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
+            if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
+                if (out.restarts < a.max_restarts && rr_cur > 0.0) {
+                    OHM_RESTART_S();
+                    continue;
+                }
+                code = kKrylovBreakRv;
+                break;
+            }
+            alpha = rho / acc1[0];
+            const double al = alpha;
+            // ---------------- CD: s = r - a v and t = A M^-1 s ----------------
+            auto s_of = [&](const KRec<T> &q) -> T {
+                return cvt<T>((double)q.r + (-al) * (double)q.v);
+            };
+            auto shat_at = [&](int j, bool slow) -> T {
+                const KRec<T> q = nxt[j];
+                double z = (double)q.c * (double)s_of(q);
+                if (slow) {
+                    const int pj = a.partner[j];
+                    if (pj >= 0) z += (double)((const T *)a.pc_part)[j] * (double)s_of(nxt[pj]);
+                }
+                return cvt<T>(z);
+            };
+            double acc3[4] = {0.0, 0.0, 0.0, 0.0};   // (s,s), (t,s), (t,t), ||W s||^2
+            auto cd_row = [&](int i, double y) {
+                const int li = i - r0;
+                const T si = s_of(rec[li]);
+                const T ti = cvt<T>(y);
+                t[li] = ti;
+                if (pair[li]) ((T *)a.s)[i] = si;
+                const double ws = wt ? w[li] * (double)si : (double)si;
+                acc3[0] += (double)si * (double)si;
+                acc3[1] += (double)ti * (double)si;
+                acc3[2] += (double)ti * (double)ti;
+                acc3[3] += ws * ws;
+            };
+            spmv_rows<LPR, Acc, T, decltype(shat_at), decltype(cd_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
+                                                                            shat_at, cd_row, a.longflag, r0);
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row, true)) return kKrylovAbort;
+            if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
+            if (sqrt(acc3[3]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
+                for (int li = threadIdx.x; li < R; li += blockDim.x) {
+                    const int i = r0 + li;
+                    const KRec<T> q = rec[li];
+                    const bool pr = pair[li] != 0;
+                    const T ph = pc_apply(i, (double)q.c, q.p, pr, pr ? nxt[a.partner[i]].p : T(0));
+                    d[li] = cvt<T>((double)d[li] + al * (double)ph);
+                }
+                code = kKrylovConverged;
+                ++it;
+                break;
+            }
+            if (!(acc3[2] > 0.0)) { code = kKrylovBreakTt; break; }
+            omega = acc3[1] / acc3[2];
+            // ---------------- E: d, r updates ----------------
+            double acc4[3] = {0.0, 0.0, 0.0};   // (r_hat, r), ||r||^2, ||W r||^2
+            for (int li = threadIdx.x; li < R; li += blockDim.x) {
+                const int i = r0 + li;
+                const KRec<T> q = rec[li];
+                const bool pr = pair[li] != 0;
+                const int pi = pr ? a.partner[i] : i;
+                const T ph = pc_apply(i, (double)q.c, q.p, pr, pr ? nxt[pi].p : T(0));
+                const T si = s_of(q);
+                const T sh = pc_apply(i, (double)q.c, si, pr, pr ? ((const T *)a.s)[pi] : T(0));
+                d[li] = cvt<T>(((double)d[li] + al * (double)ph) + omega * (double)sh);
+                const T rt = cvt<T>((double)si + (-omega) * (double)t[li]);
+                nxt[i].r = rt;
+                rec[li].r = rt;
+                const double wr = wt ? w[li] * (double)rt : (double)rt;
+                acc4[0] += (double)rhat[li] * (double)rt;
+                acc4[1] += (double)rt * (double)rt;
+                acc4[2] += wr * wr;
+            }
+            if (!g.template allreduce<3>(acc4)) return kKrylovAbort;
+            { KRec<T> *tmp = cur; cur = nxt; nxt = tmp; }
+            rho_new = acc4[0];
+            rr_cur = acc4[1];
+            const double rnorm = sqrt(acc4[2]);
+            if (!isfinite(rnorm)) { code = kKrylovNan; ++it; break; }
+            if (rnorm < abs_tol) { code = kKrylovConverged; ++it; break; }
+            if (fabs(omega) < 1e-30) { code = kKrylovBreakOmega; ++it; break; }
+            if (accept_partial && it + 1 == max_it && rnorm <= 0.5 * r0norm) {
+                code = kKrylovConverged;
+                ++it;
+                break;
+            }
+        }
+        if (code == kKrylovRunning) code = kKrylovMaxIter;
+    }
+#undef OHM_RESTART_S
+    out.iterations = it;
+    if (code == kKrylovConverged)
+        for (int li = threadIdx.x; li < R; li += blockDim.x) a.dx[r0 + li] = (double)d[li];
+    return code;
+}
+
 // One Krylov solve of J d = r64 with the configured preconditioner.
 template <typename T, int LPR, class Team>
 __device__ __forceinline__ int krylov_any(const KernelArgs &a, Team &g, double tol_floor, double inner_rtol,
                                           int max_it, bool accept_partial, KrylovOut &out) {
     if (a.precond == kPcIsai) return krylov_isai<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
+    if constexpr (std::is_same<Team, GridTeam>::value) {
+        const int code = krylov_smem<T, LPR, (LPR == 1 ? 2 : 4)>(a, g, tol_floor, inner_rtol, max_it,
+                                                                 accept_partial, out);
+        if (code != kKrylovNoSmem) return code;
+    }
     return krylov<T, LPR>(a, g, tol_floor, inner_rtol, max_it, accept_partial, out);
 }
 
