@@ -161,6 +161,7 @@ SIGNATURES = {
                                _dp, C.POINTER(AcPointInfo)]),
     "ohm_transient_run": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                     C.POINTER(NewtonParamsC), C.c_int32, _dp, C.POINTER(TransientInfo)]),
+    "ohm_transient_set_predictor": (C.c_int, [_vp, C.c_int32]),
     "ohm_solve_complex": (C.c_int, [_vp, _i64, _i64, _u32p, _u32p, _dp, _dp, _dp, C.POINTER(KrylovParams),
                                     C.POINTER(AcPointInfo)]),
     "ohm_compile": (C.c_int, [_vp, _i64, C.POINTER(C.c_int32), C.POINTER(C.c_int64), _dp, _dp,

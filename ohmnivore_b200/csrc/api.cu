@@ -163,19 +163,19 @@ static constexpr int kBlock = kSolverBlock;
 // precisions), row pointers and pair flags per row, column + value per
 // nonzero outside long rows (an estimate with a 3 % margin; a block whose
 // slice is larger works from global memory), or 0 when it cannot fit.
-int ohm_krylov_smem_bytes(KernelFn fn, int64_t n, int64_t nnz_short, int grid) {
+int ohm_krylov_smem_bytes(const void *fn, int64_t n, int64_t nnz_short, int grid) {
     if (n <= 0 || grid <= 0) return 0;
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, (const void *)fn) != cudaSuccess) return 0;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return 0;
     const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024;
     const int64_t rows = (n + grid - 1) / grid + 1;
     const int64_t nnz_blk = (int64_t)((double)std::max<int64_t>(nnz_short, 0) * (double)rows / (double)n * 1.03) + 256;
     const int64_t need = rows * (32 + 8 + 8 + 8 + 8 + 4 + 1) + nnz_blk * (8 + 4) + 16 * 16;
     if (need > avail) return 0;
-    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess)
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess)
         return 0;
     return (int)need;
 }
@@ -194,7 +194,7 @@ ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t n
     if (t.max_grid > 0) cap = std::min<int64_t>(cap, t.max_grid);
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
     // one block per SM either way: a block is 1024 threads at the register cap
-    a.smem_bytes = ohm_krylov_smem_bytes(fn, a.n, nnz - a.nnz_long, grid);
+    a.smem_bytes = ohm_krylov_smem_bytes((const void *)fn, a.n, nnz - a.nnz_long, grid);
     if (a.smem_bytes > 0) {
         int fit = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kBlock, a.smem_bytes));

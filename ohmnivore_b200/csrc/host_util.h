@@ -188,7 +188,7 @@ inline void split_long(int64_t count, const uint32_t *ptr, uint32_t min_len, uin
 // Thresholds: rows with more nonzeros than kLongRowMin, and stamp-map
 // entries with more contributions than kLongSegMin, are handled by the whole
 // team in chunks.
-constexpr uint32_t kLongRowMin = 4096, kLongRowChunk = 1024;
-constexpr uint32_t kLongSegMin = 256, kLongSegChunk = 256;
+constexpr uint32_t kLongRowMin = 4096, kLongRowChunk = 128;
+constexpr uint32_t kLongSegMin = 256, kLongSegChunk = 64;
 
 }  // namespace ohm

@@ -50,6 +50,9 @@ struct LaunchTarget {
 ohm_status ohm_launch_persistent(const LaunchTarget &t, ohm::KernelArgs &a, int64_t nnz, int *launches);
 ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, int launches);
 ohm_status ohm_check_krylov(const ohm_krylov_params *p);
+// Dynamic shared memory that lets a grid-team kernel `fn` of `grid` blocks
+// keep its Krylov slices in shared memory (sets the kernel's limit), or 0.
+int ohm_krylov_smem_bytes(const void *fn, int64_t n, int64_t nnz_short, int grid);
 // Kernel arguments of a Newton solve on a plan (validated params), its
 // context, and the launch of a plan-sized persistent kernel (api.cu).
 ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, ohm::KernelArgs &a,

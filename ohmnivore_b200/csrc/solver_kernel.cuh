@@ -298,17 +298,25 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
     }
 }
 
+// Block of the team that finishes team-shared work item q (GridTeam: block
+// q mod G; BlockTeam: its only block), and whether this block owns row i.
+template <class Team>
+__device__ __forceinline__ bool team_owns_item(const Team &g, int q) {
+    if constexpr (std::is_same<Team, GridTeam>::value) return q % g.G == g.bid;
+    else return true;
+}
+
 // Long rows (a hub node such as a supply rail, whose row holds a nonzero per
 // connected device) are skipped by spmv_rows and computed by the whole team:
-// one warp per chunk of at most a few hundred nonzeros writes a partial, a
-// team sync, then one warp per long row sums its partials in a fixed order
-// and calls f(row, y) like spmv_rows does.  With own_only, each long row is
-// finished by the block that owns it (the callback then may use that block's
-// shared memory).  Returns false if the sync gave up.
+// one warp per chunk of at most a couple of hundred nonzeros writes a partial
+// (4 nonzeros per lane, their loads issued together), a team sync, then the
+// block that owns the row sums its partials with all its threads (a fixed
+// tree, so the value does not depend on timing) and calls f(row, y) like
+// spmv_rows does, on one thread.  The callback may therefore use the owning
+// block's shared memory.  Returns false if the sync gave up.
 template <typename Acc, class Team, typename TA, typename X, typename F>
 __device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const uint32_t *__restrict__ col,
-                                          const TA *__restrict__ val, const uint8_t *rowflag, X x, F f,
-                                          bool own_only = false) {
+                                          const TA *__restrict__ val, const uint8_t *rowflag, X x, F f) {
     if (a.n_long == 0) return true;
     const int lane = threadIdx.x & 31;
     const int warp = g.gtid >> 5, nwarps = g.gstride >> 5;
@@ -316,7 +324,9 @@ __device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const ui
         const uint32_t row = a.long_row[a.long_chunk_owner[c]];
         const bool slow = rowflag != nullptr && rowflag[row] != 0;
         Acc acc = Acc(0);
-        for (uint32_t k = a.long_chunk_beg[c] + lane; k < a.long_chunk_end[c]; k += 32)
+        const uint32_t kend = a.long_chunk_end[c];
+#pragma unroll 4
+        for (uint32_t k = a.long_chunk_beg[c] + lane; k < kend; k += 32)
             acc += (Acc)val[k] * (Acc)x((int)col[k], slow);
         double s = (double)acc;
 #pragma unroll
@@ -324,15 +334,14 @@ __device__ __forceinline__ bool spmv_long(const KernelArgs &a, Team &g, const ui
         if (lane == 0) a.long_part[c] = s;
     }
     if (!g.sync()) return false;
-    const int j0 = own_only ? (int)(threadIdx.x >> 5) : warp;
-    const int js = own_only ? (int)(blockDim.x >> 5) : nwarps;
-    for (int j = j0; j < a.n_long; j += js) {
-        if (own_only && ((int)a.long_row[j] < g.r0 || (int)a.long_row[j] >= g.r1)) continue;
-        double s = 0.0;
-        for (uint32_t c = a.long_chunk_ptr[j] + lane; c < a.long_chunk_ptr[j + 1]; c += 32) s += a.long_part[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) f((int)a.long_row[j], s);
+    for (int j = 0; j < a.n_long; ++j) {
+        const int row = (int)a.long_row[j];
+        if (row < g.r0 || row >= g.r1) continue;          // uniform over the block
+        double v[1] = {0.0};
+        for (uint32_t c = a.long_chunk_ptr[j] + threadIdx.x; c < a.long_chunk_ptr[j + 1]; c += blockDim.x)
+            v[0] += a.long_part[c];
+        block_sum<1>(v, g.smem);
+        if (threadIdx.x == 0) f(row, v[0]);
     }
     return true;
 }
@@ -842,7 +851,7 @@ __device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, dou
             };
             spmv_rows<LPR, Acc, T, decltype(phat_at), decltype(ab_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
                                                                             phat_at, ab_row, a.longflag, r0);
-            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row, true)) return kKrylovAbort;
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row)) return kKrylovAbort;
             if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
             if (!(fabs(acc1[0]) >= kBreakdownRel * sqrt(rhat2 * acc1[1]))) {
                 if (out.restarts < a.max_restarts && rr_cur > 0.0) {
@@ -882,7 +891,7 @@ __device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, dou
             };
             spmv_rows<LPR, Acc, T, decltype(shat_at), decltype(cd_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
                                                                             shat_at, cd_row, a.longflag, r0);
-            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row, true)) return kKrylovAbort;
+            if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row)) return kKrylovAbort;
             if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
             if (sqrt(acc3[3]) < abs_tol) {          // early exit (bicgstab.rs:134-139)
                 for (int li = threadIdx.x; li < R; li += blockDim.x) {
@@ -1003,25 +1012,31 @@ __device__ __forceinline__ bool assemble(const KernelArgs &a, Team &g, const Run
     // stamp map: each touched slot / row = base + contributions in canonical order;
     // entries with many contributions are summed by warps in chunks first
     if (a.n_lseg) {
+        // chunks of a few dozen contributions per warp (their index and value
+        // loads issued together), then each long segment's partials summed
+        // by one block with a fixed tree
         const int lane = threadIdx.x & 31;
         for (int c = gtid >> 5; c < a.n_lseg_chunks; c += gstride >> 5) {
             const bool mat = (int)a.lseg[a.lseg_chunk_owner[c]] < a.n_mslots;
             const uint32_t *ids = mat ? a.mslot_ids : a.rrow_ids;
             const double *src = mat ? a.mstamp : a.rstamp;
             double acc = 0.0;
-            for (uint32_t j = a.lseg_chunk_beg[c] + lane; j < a.lseg_chunk_end[c]; j += 32) acc += src[ids[j]];
+            const uint32_t jend = a.lseg_chunk_end[c];
+#pragma unroll 4
+            for (uint32_t j = a.lseg_chunk_beg[c] + lane; j < jend; j += 32) acc += src[ids[j]];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane == 0) a.lseg_part[c] = acc;
         }
         OHM_SYNC_OR(false);
-        for (int q = gtid >> 5; q < a.n_lseg; q += gstride >> 5) {
-            double acc = 0.0;
-            for (uint32_t c = a.lseg_chunk_ptr[q] + lane; c < a.lseg_chunk_ptr[q + 1]; c += 32)
-                acc += a.lseg_part[c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) {
+        for (int q = 0; q < a.n_lseg; ++q) {
+            if (!team_owns_item(g, q)) continue;            // uniform over the block
+            double v[1] = {0.0};
+            for (uint32_t c = a.lseg_chunk_ptr[q] + threadIdx.x; c < a.lseg_chunk_ptr[q + 1]; c += blockDim.x)
+                v[0] += a.lseg_part[c];
+            block_sum<1>(v, g.smem);
+            const double acc = v[0];
+            if (threadIdx.x == 0) {
                 const int k = (int)a.lseg[q];
                 if (k < a.n_mslots) {
                     const uint32_t slot = a.mslot[k];

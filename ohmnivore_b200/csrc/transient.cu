@@ -48,6 +48,10 @@ struct TranArgs {
     TranDev *st;
     double *states;                    // optional: x after step s at (s - state_base) * n
     int state_base;
+    // Newton start of step s > 0: x_{n-1} (predict 0) or the linear
+    // extrapolation 2 x_{n-1} - x_{n-2} (predict 1; xpp holds x_{n-2})
+    int predict;
+    double *xpp;
 };
 
 // Source waveforms, the formulas of transient_source.rs:39-118.
@@ -130,6 +134,16 @@ __global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a
             a.b[i] = bb;
         }
         if (!g.sync()) return;
+        if (T.predict) {
+            // after every block's (C/h) x_{n-1}: own rows start from the
+            // extrapolation (x_{n-2} is known from step 1 of the run on)
+            for (int i = g.r0 + threadIdx.x; i < g.r1; i += blockDim.x) {
+                const double xp = a.x[i];
+                if (s > 0) a.x[i] = 2.0 * xp - T.xpp[i];
+                T.xpp[i] = xp;
+            }
+            if (!g.sync()) return;
+        }
         // ---- Newton on the companion system, from x_{n-1} ----
         RunOut o;
         RunCfg c{0.0, 1.0, 0.0, a.max_outer, a.max_krylov, false};
@@ -436,6 +450,8 @@ struct ohm_transient {
     AdaptDev *ad_st = nullptr;
     double *times = nullptr;
     int64_t times_cap = 0;
+    int predict = 0;                            // ohm_transient_set_predictor
+    double *xpp = nullptr;                      // x_{n-2} for the predictor
 
     template <typename T>
     cudaError_t put(T **dst, const T *h, size_t count) {
@@ -579,8 +595,9 @@ static ohm_status tran_args(ohm_transient *t, double *x_dev, const ohm_newton_pa
 }
 
 // Cooperative grid of a transient kernel: up to two blocks per SM, no more
-// blocks than rows or devices need.
-static ohm_status tran_grid(ohm_transient *t, const void *fn, const KernelArgs &a, int &grid) {
+// blocks than rows or devices need; and the dynamic shared memory of its
+// Krylov slices (a.smem_bytes, 0 when they do not fit).
+static ohm_status tran_grid(ohm_transient *t, const void *fn, KernelArgs &a, int &grid) {
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0));
     if (per_sm < 1) return ohm_fail(OHM_ERR_CUDA, "transient kernel does not fit on an SM");
@@ -588,6 +605,13 @@ static ohm_status tran_grid(ohm_transient *t, const void *fn, const KernelArgs &
     int64_t want = (t->n + kSolverBlock - 1) / kSolverBlock;
     want = std::max<int64_t>(want, ((int64_t)a.nd + a.nq + a.nm + kSolverBlock - 1) / kSolverBlock);
     grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * t->ctx->num_sms));
+    a.smem_bytes = ohm_krylov_smem_bytes(fn, t->n, t->nnz - a.nnz_long, grid);
+    if (a.smem_bytes > 0) {
+        int fit = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kSolverBlock, a.smem_bytes));
+        if (fit < 1) a.smem_bytes = 0;
+        else grid = (int)std::min<int64_t>(grid, (int64_t)fit * t->ctx->num_sms);
+    }
     return OHM_OK;
 }
 
@@ -620,7 +644,7 @@ static cudaError_t tran_launch(ohm_ctx *c, TranFn fn, int grid, const KernelArgs
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kSolverBlock);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = (size_t)a.smem_bytes;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -643,6 +667,16 @@ static ohm_status tran_status(ohm_transient *t, double t0, double h, TranDev &d)
                         : (d.status == kErrNewtonNumerical ? OHM_ERR_NEWTON_NUMERICAL : OHM_ERR_NEWTON_NOT_CONVERGED),
                         "transient step %d at t = %.6e failed (status %d, krylov code %d)", d.failed_step,
                         t0 + (d.failed_step + 1) * h, d.status, d.kcode);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_transient_set_predictor(ohm_transient *t, int32_t order) {
+    if (!t || order < 0 || order > 1) return ohm_fail(OHM_ERR_INVALID_ARG, "predictor order must be 0 or 1");
+    if (order == 1 && !t->xpp) {
+        cudaError_t e = t->put(&t->xpp, (const double *)nullptr, (size_t)t->n);
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "predictor buffer: %s", cudaGetErrorString(e));
+    }
+    t->predict = order;
     return OHM_OK;
 }
 
@@ -675,6 +709,8 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
     ohm_status st = tran_prepare(t, x_dev, h, np, a, T, fn, grid, G);
     if (st != OHM_OK) return st;
     T.t0 = t0;
+    T.predict = t->predict;
+    T.xpp = t->xpp;
     const int64_t nnz = t->nnz;
     const int n_launch = (n_steps + steps_per_launch - 1) / steps_per_launch;
     auto enqueue = [&]() -> cudaError_t {
@@ -804,6 +840,7 @@ extern "C" ohm_status ohm_transient_run_adaptive(ohm_transient *t, double *x_dev
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(grid);
         cfg.blockDim = dim3(kSolverBlock);
+        cfg.dynamicSmemBytes = (size_t)a.smem_bytes;
         cfg.stream = c->stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;

@@ -741,6 +741,14 @@ class Transient:
             _raise(st)
         return {"R": gr, "C": gc, "Is": gd, "VTO": gvto, "KP": gkp}, info.as_dict()
 
+    def set_predictor(self, order: int):
+        """Newton start of each fixed step after the first: 0 = x_{n-1}, 1 = the
+        linear extrapolation 2 x_{n-1} - x_{n-2} (same BE solution, usually
+        fewer Newton iterations)."""
+        st = self.ctx.lib.ohm_transient_set_predictor(self._h, int(order))
+        if st != _lib.OK:
+            _raise(st)
+
     def run(self, x_dev_ptr: int, t0: float, h: float, n_steps: int, params: NewtonParams | None = None,
             steps_per_launch: int = 100, graph: bool = True, check: bool = True):
         """Advance x (device pointer, x(t0) in, x(t0 + n_steps h) out).

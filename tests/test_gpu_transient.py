@@ -27,11 +27,12 @@ def _wave_err(w, ref):
     return float(np.max(np.abs(w - ref)) / max(np.max(np.abs(ref)), 1e-300))
 
 
-def _run(s, x0, t0, h, n, probes, **kw):
+def _run(s, x0, t0, h, n, probes, predictor=0, **kw):
     import torch
     ctx = S.default_context()
     plan = S.NewtonPlan(s, ctx)
     tr = S.Transient(plan, probes)
+    tr.set_predictor(predictor)
     try:
         x = torch.from_numpy(np.ascontiguousarray(x0, dtype=np.float64)).cuda()
         params = kw.pop("params", _params())
@@ -155,6 +156,12 @@ def test_supply_rail_chain_dc_and_transient():
     wave, _, _ = _run(s, ref_dc, 0.0, 5e-12, 30, probes, steps_per_launch=30)
     _, ref, _ = tref.be_transient(s, ref_dc, 0.0, 5e-12, 30, probes)
     assert _wave_err(wave, ref) < 1e-9
+    # the linear predictor starts each step's Newton elsewhere and reaches
+    # the same backward-Euler solutions, in fewer iterations
+    wave_p, _, info_p = _run(s, ref_dc, 0.0, 5e-12, 30, probes, predictor=1, steps_per_launch=7)
+    _, _, info_0 = _run(s, ref_dc, 0.0, 5e-12, 30, probes, steps_per_launch=7)
+    assert _wave_err(wave_p, ref) < 1e-9
+    assert info_p["newton_iterations"] <= info_0["newton_iterations"]
 
 
 def test_failed_step_is_reported():
