@@ -64,7 +64,8 @@ def parse():
     p.add_argument("--ladder-nodes", type=int, default=10_000,
                    help="resistor-ladder nodes of the linear DC measurement (0 skips it)")
     p.add_argument("--sections", default="dc,ladder,batch,transient,adjoint,grid,compile,ac",
-                   help="comma list of dc (the headline), ladder, batch, transient, adjoint, grid, compile, ac; a run "
+                   help="comma list of dc (the headline), ladder, batch, transient, adjoint, grid, compile, ac, "
+                        "and gradcheck (not a default: ~130 forward transients of the 1M-row mesh); a run "
                         "without dc "
                         "prints only the chosen sections (for profiling small cases); 'spmv' alone "
                         "runs the backend SpMV measurement")
@@ -269,6 +270,8 @@ def main():
             line["compile"] = guarded(compile_section, args, S, ctx, stream, barrier, world, rank, local_rank)
         if "ac" in sections and args.ac_rows > 0:
             line["ac"] = guarded(ac_section, args, S, ctx, stream, barrier, world, rank, local_rank)
+        if "gradcheck" in sections and args.adjoint_rows > 0:
+            line["gradcheck"] = guarded(gradcheck_section, args, S, ctx, stream, barrier, world, rank, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         plan.close()
@@ -561,7 +564,8 @@ def batch_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import newton_ref
         ev, ei = 0.0, 0.0
-        for i in sample[::2]:
+        check = sorted({int(order[(k * len(order)) // 64]) for k in range(64)})   # size-stratified
+        for i in check:
             s = systems[i]
             ref, _ = newton_ref.dc_operating_point(s)
             nn = slice(0, s.n_nodes)
@@ -569,16 +573,19 @@ def batch_section(args, S, ctx, stream, barrier, world, rank, local_rank):
             ev = max(ev, float(np.max(np.abs(xs[i][nn] - ref[nn])) / np.max(np.abs(ref[nn]))))
             if s.size > s.n_nodes:
                 ei = max(ei, float(np.max(np.abs(xs[i][br] - ref[br])) / max(np.max(np.abs(ref[br])), 1e-300)))
-        out["rel_err_vs_oracle"] = {"voltages": ev, "currents": ei, "instances": len(sample[::2])}
+        out["rel_err_vs_oracle"] = {"voltages": ev, "currents": ei, "instances": len(check),
+                                    "sample": "size-stratified: every (len/64)-th instance by size"}
     return out
 
 
 def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     """CMOS inverter chain (100,000 stages, 200,000 level-1 MOSFETs, 10 fF
     loads, PULSE input 0-1.8 V, 50 ps edges, 2 ns period): 2000 backward-Euler
-    steps of 5 ps, a Newton solve per step, all steps on the device, replayed
+    steps of 5 ps, a Newton solve per step started from the linear
+    extrapolation of the last two steps, all steps on the device, replayed
     as one CUDA graph of 20 persistent launches.  Precision: FP32 Krylov bulk
-    with FP64 residual / update (and the plain FP64 path beside it)."""
+    with FP64 residual / update (and the plain FP64 path beside it).  The
+    first 50 steps are checked against the oracle (LU Newton per step)."""
     import torch
     from ohmnivore_b200 import circuits, mna
     stages, nsteps, h = args.tran_stages, args.tran_steps, 5e-12
@@ -597,6 +604,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     xdc = x.clone()
     probes = [sysm.node_index(k) for k in (2, 3, 4, 5, 102, 1002, 2 + stages)]
     tr = S.Transient(plan, probes)
+    tr.set_predictor(1)
 
     def step_params(mixed):
         return S.NewtonParams(max_iterations=50, abs_tol=1e-9, bicgstab_max_iterations=20000,
@@ -626,6 +634,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     res = {"workload": f"CMOS inverter chain, {stages} stages ({2 * stages} MOSFETs), {nsteps} BE steps of 5 ps",
            "value": world * nsteps / (ms_m * 1e-3), "unit": "timesteps/s", "ms_full_run": ms_m,
            "precision": "FP32 Krylov bulk, FP64 device evaluation / residual / update",
+           "newton_start": "linear extrapolation 2 x_{n-1} - x_{n-2} (ohm_transient_set_predictor)",
            "newton_iterations": info_m["newton_iterations"], "krylov_iterations": info_m["krylov_iterations"],
            "fp64_fallbacks": info_m["fp64_fallbacks"], "kernel_launches": info_m["launches"],
            "cuda_graph": bool(info_m["graph"]), "clocks": clk.summary(),
@@ -656,7 +665,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
         from oracle import newton_ref, transient_ref
         xd = xdc.cpu().numpy()
         ref_dc, _ = newton_ref.newton(sysm, x0=xd)
-        k = 3
+        k = 50
         t0 = time.perf_counter()
         _, ref_wave, _ = transient_ref.be_transient(sysm, ref_dc, 0.0, h, k, probes)
         cpu_s = time.perf_counter() - t0
@@ -900,8 +909,9 @@ def adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     """Adjoint sensitivities on the 1000x1000 RC mesh with diodes at 5% of the
     nodes (seed 4), driven by a 1 V step through 50 ohm: the gradient of one
     node voltage at t = 1 ns (500 BE steps of 2 ps) w.r.t. every R, C and Is,
-    by the checkpointed transient adjoint (checkpoints every 50 steps, DC
-    start included).  Outputs: the corner opposite the drive (the configured
+    by the transient adjoint (every forward state kept in HBM, 500 x 1 M
+    doubles = 4 GB, so the reverse sweep recomputes nothing; DC start
+    included).  Outputs: the corner opposite the drive (the configured
     one) and node (10, 10) near the drive, where the response is nonzero;
     GPU central differences (relative step 1e-6) on the three resistors with
     the largest gradients of the latter."""
@@ -944,10 +954,10 @@ def adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank):
         w = np.zeros(sysm.size)
         w[row] = 1.0
         with ClockSampler(local_rank) as clk:
-            ms, (g, info) = ev_time(lambda: tr.adjoint(x.data_ptr(), 0.0, h, nsteps, w, comps, pn, 50))
+            ms, (g, info) = ev_time(lambda: tr.adjoint(x.data_ptr(), 0.0, h, nsteps, w, comps, pn, 0))
         out[name] = {"output_V": info["output"], "adjoint_ms": ms, "linear_solves": info["linear_solves"],
                      "krylov_iterations": info["krylov_iterations"],
-                     "max_abs_grad": {k: float(np.max(np.abs(v))) for k, v in g.items()},
+                     "max_abs_grad": {k: float(np.max(np.abs(v))) for k, v in g.items() if len(v)},
                      "nonzero_grads": {k: int(np.count_nonzero(v)) for k, v in g.items()},
                      "clocks": clk.summary()}
         if name == "node_10_10":
@@ -990,6 +1000,126 @@ def adjoint_section(args, S, ctx, stream, barrier, world, rank, local_rank):
                                                          f"timed and scaled to {nsteps + 1} solves, no forward pass"}
     tr.close()
     plan.close()
+    return res
+
+
+def gradcheck_section(args, S, ctx, stream, barrier, world, rank, local_rank):
+    """Full-size check of the config-5 gradient (not in the default sections:
+    ~130 forward transients of the 1M-row mesh): the transient adjoint of
+    V(node (10, 10)) at t = 1 ns (500 BE steps of 2 ps) against GPU central
+    differences (relative step 1e-6, over the values actually used) on a
+    seeded subset of 64 parameters, 24 R, 24 C and 16 Is, drawn among those
+    whose relative sensitivity |p dO/dp| is at least 1e-2 of the largest of
+    their kind (a 1e-6 change of a weaker one moves the output by less than
+    the forward solves resolve).  Every solve stops at max|dx| < 1e-13 V.
+    The output's dependence on Is is weak (|Is dO/dIs| <= ~3e-9 V), so Is
+    takes a relative step of 1e-3; a 1e-6 step moves the output by ~1e-14 V.
+    R perturbs the plan's conductance base, C a new transient object's C
+    values, Is a new plan's descriptors (f32, as the descriptors store it)."""
+    import copy
+    import torch
+    from ohmnivore_b200 import circuits, mna
+    rows, nsteps, h = args.adjoint_rows, 500, 2e-12
+    ckt = circuits.rc_diode_mesh(rows, rows, seed=4)
+    sysm = mna.compile_circuit(ckt)
+    comps = S.ComponentTable(ckt, sysm)
+    pn = S.NewtonParams(max_iterations=100, abs_tol=1e-13, bicgstab_max_iterations=20000,
+                        bicgstab_tolerance=1e-15, inner_rtol=1e-8)
+    plan = S.NewtonPlan(sysm, ctx)
+    dev = f"cuda:{local_rank}"
+    x = torch.zeros(sysm.size, dtype=torch.float64, device=dev)
+    plan.newton_device(x.data_ptr(), pn)
+    near = sysm.node_index(2 + 10 * rows + 10)
+    tr = S.Transient(plan, [near])
+    w = np.zeros(sysm.size)
+    w[near] = 1.0
+    t0 = time.perf_counter()
+    try:
+        g, info = tr.adjoint(x.data_ptr(), 0.0, h, nsteps, w, comps, pn, 0)
+    except S.OhmnivoreError as e:
+        raise RuntimeError(f"adjoint: {e}") from e
+    adj_s = time.perf_counter() - t0
+    x0 = x.clone()
+
+    def forward(p, t):
+        xs = torch.zeros(sysm.size, dtype=torch.float64, device=dev)
+        try:
+            p.newton_device(xs.data_ptr(), pn)
+        except S.OhmnivoreError as e:
+            raise RuntimeError(f"forward DC: {e}") from e
+        try:
+            return float(t.run(xs.data_ptr(), 0.0, h, nsteps, pn, steps_per_launch=100)[-1, 0])
+        except S.OhmnivoreError as e:
+            raise RuntimeError(f"forward transient: {e} {t.last_info}") from e
+
+    rng = np.random.default_rng(7)
+    picks = {}
+    pval = {"R": comps.r_ohms, "C": comps.c_farads,
+            "Is": sysm.diode_descriptors["is_val"].astype(np.float64)}
+    step = {"R": 1e-6, "C": 1e-6, "Is": 1e-3}
+    for kind, cnt in (("R", 24), ("C", 24), ("Is", 16)):
+        rs = np.abs(g[kind] * pval[kind])
+        cand = np.flatnonzero(rs >= 1e-2 * np.max(rs))
+        picks[kind] = np.sort(rng.choice(cand, size=min(cnt, len(cand)), replace=False))
+    gv = sysm.g.val.copy()
+    res = {"workload": f"RC-diode mesh {rows}x{rows} ({sysm.size} unknowns), d V(node 10,10)(1 ns)/dp, "
+                       f"{nsteps} BE steps of 2 ps", "adjoint_s": adj_s, "output_V": info["output"]}
+    t0 = time.perf_counter()
+    for kind in ("R", "C", "Is"):
+        errs = []
+        for j in picks[kind]:
+            outs, vals = [], []
+            for sign in (1, -1):
+                if kind == "R":
+                    r0_ = comps.r_ohms[j]
+                    r1_ = r0_ * (1 + sign * step["R"])
+                    dg = 1.0 / r1_ - 1.0 / r0_
+                    a_, b_ = int(comps.r_a[j]), int(comps.r_b[j])
+                    v2 = gv.copy()
+                    for (ri, ci, sg) in ((a_, a_, 1), (b_, b_, 1), (a_, b_, -1), (b_, a_, -1)):
+                        if ri >= 0 and ci >= 0:
+                            v2[sysm.g.value_index(ri, ci)] += sg * dg
+                    plan.set_base(v2)
+                    outs.append(forward(plan, tr))
+                    vals.append(r1_)
+                elif kind == "C":
+                    c0_ = comps.c_farads[j]
+                    c1_ = c0_ * (1 + sign * step["C"])
+                    s2 = copy.copy(sysm)
+                    cc = copy.copy(sysm.c)
+                    cc.val = sysm.c.val.copy()
+                    a_, b_ = int(comps.c_a[j]), int(comps.c_b[j])
+                    for (ri, ci, sg) in ((a_, a_, 1), (b_, b_, 1), (a_, b_, -1), (b_, a_, -1)):
+                        if ri >= 0 and ci >= 0:
+                            cc.val[cc.value_index(ri, ci)] += sg * (c1_ - c0_)
+                    s2.c = cc
+                    plan.sysm = s2
+                    t2 = S.Transient(plan, [near])
+                    plan.sysm = sysm
+                    outs.append(forward(plan, t2))
+                    t2.close()
+                    vals.append(c1_)
+                else:
+                    s2 = copy.copy(sysm)
+                    dd = sysm.diode_descriptors.copy()
+                    dd["is_val"][j] = np.float32(float(dd["is_val"][j]) * (1 + sign * step["Is"]))
+                    s2.diode_descriptors = dd
+                    p2 = S.NewtonPlan(s2, ctx)
+                    t2 = S.Transient(p2, [near])
+                    outs.append(forward(p2, t2))
+                    t2.close()
+                    p2.close()
+                    vals.append(float(dd["is_val"][j]))
+            plan.set_base(gv)
+            fd = (outs[0] - outs[1]) / (vals[0] - vals[1])
+            errs.append(abs(g[kind][j] - fd) / max(abs(fd), 1e-3 * float(np.max(np.abs(g[kind])))))
+        res[kind] = {"parameters": len(picks[kind]), "relative_step": step[kind],
+                     "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+                     "within_1e-6": int(sum(e <= 1e-6 for e in errs))}
+    res["fd_wall_s"] = time.perf_counter() - t0
+    tr.close()
+    plan.close()
+    del x0
     return res
 
 

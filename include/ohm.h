@@ -101,7 +101,10 @@ typedef struct {                 /* BiCgStabParams (src/solver/bicgstab.rs:14-27
                                     0 = the reference's breakdown error; default 50 */
     int32_t fp32_max_iterations; /* mixed: iterations of an FP32 attempt before the solve is
                                     redone in FP64 (unless it reduced ||r|| by 2x); default 600 */
-    int32_t reserved;
+    int32_t fp32_min_eta_exp;    /* mixed Newton: a linear solve whose inner tolerance is below
+                                    10^-fp32_min_eta_exp goes straight to FP64 (FP32 BiCGSTAB
+                                    stagnates short of tight tolerances on ill-conditioned
+                                    systems); 0 = always try FP32 first (default) */
 } ohm_krylov_params;
 
 typedef enum {
@@ -432,7 +435,9 @@ ohm_status ohm_transient_run_adaptive(ohm_transient *tr, double *x_inout_device,
  * step back-stamps as above plus capacitor (a, b, C):
  * -(lambda_a - lambda_b)((v_a - v_b)_n - (v_a - v_b)_{n-1}) / h.  The forward
  * states are recomputed segment by segment from checkpoints taken every
- * `checkpoint_every` steps.  Gradients accumulate in FP64 on the device.
+ * `checkpoint_every` steps, or, with checkpoint_every = 0, every state is
+ * kept (n_steps x n doubles of device memory) and nothing is recomputed.
+ * Gradients accumulate in FP64 on the device.
  * When x_0 is identically zero (all sources off at t0) every DC term is zero
  * and the DC start solve is skipped (info->linear_solves = n_steps). */
 typedef struct {

@@ -25,7 +25,7 @@ class KrylovParams(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("tolerance", C.c_double), ("precision", C.c_int32),
                 ("precond", C.c_int32), ("inner_rtol", C.c_double), ("max_refinements", C.c_int32),
                 ("max_restarts", C.c_int32), ("fp32_max_iterations", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("fp32_min_eta_exp", C.c_int32)]
 
 
 class Components(C.Structure):

@@ -50,7 +50,7 @@ extern "C" void ohm_krylov_params_default(ohm_krylov_params *p) {
     p->max_refinements = 1;
     p->max_restarts = 50;
     p->fp32_max_iterations = 600;
-    p->reserved = 0;
+    p->fp32_min_eta_exp = 0;
 }
 
 extern "C" void ohm_newton_params_default(ohm_newton_params *p) {
@@ -771,6 +771,7 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     a.inner_rtol = mixed ? (kp.inner_rtol > 0.0 ? kp.inner_rtol : 1e-4) : kp.inner_rtol;
     a.max_restarts = std::max(0, kp.max_restarts);
     a.fp32_max_iterations = kp.fp32_max_iterations > 0 ? kp.fp32_max_iterations : kp.max_iterations;
+    a.fp32_min_eta = kp.fp32_min_eta_exp > 0 ? std::pow(10.0, -(double)kp.fp32_min_eta_exp) : 0.0;
     a.forcing = np->forcing;
     a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
     a.trace = p->trace;
@@ -810,6 +811,11 @@ ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double
 }
 
 ohm_ctx *ohm_plan_context(ohm_plan *p) { return p ? p->ctx : nullptr; }
+
+cudaError_t ohm_plan_restore_rhs(ohm_plan *p) {
+    if (!p || p->n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(p->b, p->base_b, p->n * sizeof(double), cudaMemcpyDeviceToDevice, p->ctx->stream);
+}
 
 extern "C" ohm_status ohm_plan_newton_device(ohm_plan *p, double *x_dev, const ohm_newton_params *np,
                                              ohm_solve_info *info) {

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -257,6 +258,7 @@ static ohm_status batch_args(ohm_batch *b, double *x_dev, const ohm_newton_param
     a.eta_max = np->eta_max > 0.0 ? np->eta_max : 0.5;
     a.fp32_max_iterations = np->krylov.fp32_max_iterations > 0 ? np->krylov.fp32_max_iterations
                                                                : np->krylov.max_iterations;
+    a.fp32_min_eta = np->krylov.fp32_min_eta_exp > 0 ? std::pow(10.0, -(double)np->krylov.fp32_min_eta_exp) : 0.0;
     a.max_restarts = std::max(0, np->krylov.max_restarts);
     a.continuation = np->continuation ? (1 | (np->continuation & OHM_CONT_TEST_PSEUDO)) : 0;
     return OHM_OK;

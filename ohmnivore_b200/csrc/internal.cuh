@@ -58,6 +58,10 @@ int ohm_krylov_smem_bytes(const void *fn, int64_t n, int64_t nnz_short, int grid
 ohm_status ohm_plan_kernel_args(ohm_plan *p, const ohm_newton_params *np, double *x_dev, ohm::KernelArgs &a,
                                 int64_t *nnz);
 ohm_ctx *ohm_plan_context(ohm_plan *p);
+// Copies the plan's base rhs back into its assembled rhs (a Newton solve
+// re-stamps only the rows that devices touch, so a run that assembled
+// another rhs into the plan, such as a transient step, must restore it).
+cudaError_t ohm_plan_restore_rhs(ohm_plan *p);
 // J(x) values of a plan's system at a device x, on base values base_vals_dev
 // (the plan's conductance base when null), written to J_out (nnz doubles).
 ohm_status ohm_plan_jacobian_device(ohm_plan *p, const double *x_dev, const double *base_vals_dev, double *J_out);

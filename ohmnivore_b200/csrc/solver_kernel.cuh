@@ -161,6 +161,7 @@ struct KernelArgs {
     int forcing;                // 1: Eisenstat-Walker inner tolerance, floor inner_rtol
     double eta_max;             // Eisenstat-Walker upper bound
     int fp32_max_iterations;    // mixed: iteration cap of an FP32 attempt before FP64
+    double fp32_min_eta;        // mixed Newton: inner tolerances below this go straight to FP64
     int max_restarts;           // restarts with r_hat = r after a breakdown
     double *trace;              // optional per-outer-iteration record (kTraceCols doubles)
     int trace_cap;
@@ -1179,7 +1180,7 @@ __device__ __forceinline__ bool newton_run(const KernelArgs &a, Team &g, const R
         }
         KrylovOut ko{0, 0};
         int it32 = 0, it64 = 0;
-        if (a.mixed) {
+        if (a.mixed && !(a.newton && eta < a.fp32_min_eta)) {
             kcode = krylov_any<float, LPR>(a, g, floor_tol, eta, min(a.fp32_max_iterations, cfg.max_krylov), true, ko);
             if (kcode == kKrylovAbort) return false;
             it32 = ko.iterations;

@@ -746,6 +746,7 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
     }
     // restore the plan's assembled system to its conductance base
     restore_kernel<<<steps_grid(nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, nnz);
+    CUDA_TRY(ohm_plan_restore_rhs(t->plan));
     CUDA_TRY(cudaGetLastError());
     TranDev d{};
     const ohm_status rs = tran_status(t, t0, h, d);
@@ -851,6 +852,7 @@ extern "C" ohm_status ohm_transient_run_adaptive(ohm_transient *t, double *x_dev
     }
     // restore the plan's assembled system to its conductance base
     restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
+    CUDA_TRY(ohm_plan_restore_rhs(t->plan));
     CUDA_TRY(cudaGetLastError());
     AdaptDev d{};
     unsigned int words[4] = {0, 0, 0, 0};
@@ -1142,14 +1144,17 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
                                             double *d_out_dis, double *d_out_dvto, double *d_out_dkp,
                                             ohm_adjoint_info *info) {
     if (!t || !x0_dev || !np || !w_host || !kp) return ohm_fail(OHM_ERR_INVALID_ARG, "null argument");
-    if (!(h > 0.0) || n_steps < 1 || checkpoint_every < 1)
-        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 1, checkpoint_every >= 1");
+    if (!(h > 0.0) || n_steps < 1 || checkpoint_every < 0)
+        return ohm_fail(OHM_ERR_INVALID_ARG, "need h > 0, n_steps >= 1, checkpoint_every >= 0");
     if (np->continuation || np->krylov.precond == OHM_PRECOND_ISAI1)
         return ohm_fail(OHM_ERR_INVALID_ARG, "transient steps use block Jacobi or Jacobi, no continuation");
     ohm_ctx *c = t->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
     const int64_t n = t->n;
-    const int K = checkpoint_every;
+    // checkpoint_every = 0: the forward pass keeps every state (n_steps x n
+    // doubles) and the reverse sweep recomputes nothing
+    const bool keep_all = checkpoint_every == 0;
+    const int K = keep_all ? n_steps : checkpoint_every;
     const int nseg = (n_steps + K - 1) / K;
     AdjointCtx A;
     double *x = nullptr, *ck = nullptr, *S = nullptr;
@@ -1196,6 +1201,10 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
     T.t0 = t0;
     T.n_probes = 0;
     int launches = 0;
+    if (keep_all) {
+        T.states = S;
+        T.state_base = 0;
+    }
     for (int sg = 0; sg < nseg; ++sg) {
         CUDA_TRY(cudaMemcpyAsync(ck + (size_t)sg * n, x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         CUDA_TRY(tran_launch(c, fn, grid, a, T, sg * K, std::min(n_steps, (sg + 1) * K)));
@@ -1211,13 +1220,16 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
     const double inv_h = 1.0 / h;
     for (int sg = nseg - 1; st == OHM_OK && sg >= 0; --sg) {
         const int s0 = sg * K, s1 = std::min(n_steps, (sg + 1) * K);
-        // recompute x_{s0+1} .. x_{s1} from the checkpoint x_{s0}
-        CUDA_TRY(cudaMemcpyAsync(x, ck + (size_t)sg * n, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-        T.states = S;
-        T.state_base = s0;
-        CUDA_TRY(tran_launch(c, fn, grid, a, T, s0, s1));
-        ++launches;
-        st = tran_status(t, t0, h, d);
+        if (!keep_all) {
+            // recompute x_{s0+1} .. x_{s1} from the checkpoint x_{s0}
+            CUDA_TRY(cudaMemcpyAsync(x, ck + (size_t)sg * n, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     c->stream));
+            T.states = S;
+            T.state_base = s0;
+            CUDA_TRY(tran_launch(c, fn, grid, a, T, s0, s1));
+            ++launches;
+            st = tran_status(t, t0, h, d);
+        }
         for (int s = s1 - 1; st == OHM_OK && s >= s0; --s) {
             // step s maps x_s (state index s, or the checkpoint) to x_{s+1}
             const double *xn = S + (size_t)(s - s0) * n;
@@ -1249,6 +1261,7 @@ extern "C" ohm_status ohm_transient_adjoint(ohm_transient *t, const double *x0_d
         if (st != OHM_OK) st = ohm_fail(st, "adjoint solve of the DC start: %s", ohm_last_error());
     }
     restore_kernel<<<steps_grid(t->nnz), 256, 0, c->stream>>>(G, a.vals64, a.vals32, t->nnz);
+    CUDA_TRY(ohm_plan_restore_rhs(t->plan));
     if (st == OHM_OK) st = A.download(d_out_dr, d_out_dc, d_out_dis, d_out_dvto, d_out_dkp, nullptr);
     if (info) {
         std::memset(info, 0, sizeof *info);

@@ -93,6 +93,7 @@ class BiCgStabParams:
     max_refinements: int = 1
     max_restarts: int = 50
     fp32_max_iterations: int = 600
+    fp32_min_eta_exp: int = 0
 
     def to_c(self) -> _lib.KrylovParams:
         p = _lib.KrylovParams()
@@ -105,6 +106,7 @@ class BiCgStabParams:
         p.max_refinements = int(self.max_refinements)
         p.max_restarts = int(self.max_restarts)
         p.fp32_max_iterations = int(self.fp32_max_iterations)
+        p.fp32_min_eta_exp = int(self.fp32_min_eta_exp)
         return p
 
 
@@ -123,6 +125,7 @@ class NewtonParams:
     forcing: int = 0              # 0 constant inner_rtol, 1 Eisenstat-Walker
     eta_max: float = 0.5
     fp32_max_iterations: int = 600
+    fp32_min_eta_exp: int = 0     # mixed: inner tolerances below 10^-k go straight to FP64 (0 = off)
     continuation: int = 0         # 1: reference DC strategy on failure (src/analysis/dc.rs:60-290);
                                   # | CONT_TEST_PSEUDO (testing): force the pseudo-transient stage
     n_nodes: int = 0              # node rows; filled from the system by NewtonPlan / NewtonBatch
@@ -135,7 +138,8 @@ class NewtonParams:
         p.rel_tol = float(self.rel_tol)
         p.krylov = BiCgStabParams(self.bicgstab_max_iterations, self.bicgstab_tolerance,
                                   self.precision, self.precond, self.inner_rtol,
-                                  fp32_max_iterations=self.fp32_max_iterations).to_c()
+                                  fp32_max_iterations=self.fp32_max_iterations,
+                                  fp32_min_eta_exp=self.fp32_min_eta_exp).to_c()
         p.forcing = int(self.forcing)
         p.eta_max = float(self.eta_max)
         p.continuation = int(self.continuation)

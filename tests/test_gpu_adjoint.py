@@ -125,11 +125,12 @@ def test_transient_adjoint_matches_central_differences():
 
 def test_checkpoint_interval_does_not_change_gradients():
     """Recomputing segments from checkpoints reproduces the forward states
-    exactly, so every interval gives bit-identical gradients."""
+    exactly, so every interval gives bit-identical gradients, the same as
+    keeping every state (checkpoint_every = 0)."""
     _, s, comps, probe = _transient_case()
     x0, _ = newton_ref.newton(s)
     w = _probe_w(s, probe)
-    gs = [_gpu_transient_adjoint(s, comps, x0, 24, w, k)[0] for k in (1, 5, 24)]
+    gs = [_gpu_transient_adjoint(s, comps, x0, 24, w, k)[0] for k in (0, 1, 5, 24)]
     for g in gs[1:]:
         for k in ("R", "C", "Is"):
             np.testing.assert_array_equal(g[k], gs[0][k])

@@ -202,3 +202,36 @@ def test_capacitance_off_pattern_rejected():
         assert st == _lib.ERR_COMPILE and not h.value
     finally:
         plan.close()
+
+
+def test_dc_solve_after_transient_on_the_same_plan():
+    """A transient run assembles the backward-Euler rhs into the plan; the
+    plan's rhs is restored afterwards, so a DC solve on the same plan (which
+    re-stamps only the rows that devices touch) gives the same operating
+    point, bit for bit, as before the run; likewise after the adaptive run
+    and the transient adjoint."""
+    import torch
+    s = mna.compile_circuit(_rc_sources_circuit())
+    plan = S.NewtonPlan(s)
+    tr = S.Transient(plan, [0])
+    try:
+        def dc():
+            x = torch.zeros(s.size, dtype=torch.float64, device="cuda")
+            plan.newton_device(x.data_ptr(), _params())
+            return x.cpu().numpy()
+        x_dc = dc()
+        x = torch.from_numpy(x_dc).cuda()
+        tr.run(x.data_ptr(), 0.0, 1e-10, 40, _params())
+        np.testing.assert_array_equal(dc(), x_dc)
+        x = torch.from_numpy(x_dc).cuda()
+        tr.run_adaptive(x.data_ptr(), 1e-10, 4e-9, 0.0, _params())
+        np.testing.assert_array_equal(dc(), x_dc)
+        comps = S.ComponentTable(_rc_sources_circuit(), s)
+        x = torch.from_numpy(x_dc).cuda()
+        w = np.zeros(s.size)
+        w[0] = 1.0
+        tr.adjoint(x.data_ptr(), 0.0, 1e-10, 20, w, comps, _params(), 5)
+        np.testing.assert_array_equal(dc(), x_dc)
+    finally:
+        tr.close()
+        plan.close()
