@@ -61,6 +61,8 @@ def parse():
                    help="RC mesh size of the AC sweep measurement (0 skips it)")
     p.add_argument("--grid-rows", type=int, default=1000,
                    help="mesh size of the large-grid DC measurement (0 skips it)")
+    p.add_argument("--compile-small", action="store_true",
+                   help="compile section on 100x100 meshes and a 2,000-stage chain (for profiling)")
     p.add_argument("--ladder-nodes", type=int, default=10_000,
                    help="resistor-ladder nodes of the linear DC measurement (0 skips it)")
     p.add_argument("--sections", default="dc,ladder,batch,transient,adjoint,grid,compile,ac",
@@ -690,6 +692,10 @@ def compile_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     work = [("diode mesh 500x500 (headline)", lambda: circuits.diode_mesh(500, 500, seed=1)),
             ("RC-diode mesh 1000x1000", lambda: circuits.rc_diode_mesh(1000, 1000, seed=4)),
             ("inverter chain, 100,000 stages", lambda: circuits.inverter_chain(stages=100_000, seed=2))]
+    if args.compile_small:
+        work = [("diode mesh 100x100", lambda: circuits.diode_mesh(100, 100, seed=1)),
+                ("RC-diode mesh 100x100", lambda: circuits.rc_diode_mesh(100, 100, seed=4)),
+                ("inverter chain, 2,000 stages", lambda: circuits.inverter_chain(stages=2000, seed=2))]
     S.compile_circuit_device(circuits.diode_mesh(8, 8, seed=1), ctx)        # module load, memory cache
     res = {}
     for name, mk in work:
