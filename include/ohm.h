@@ -169,6 +169,19 @@ ohm_status ohm_ctx_destroy(ohm_ctx *ctx);
 ohm_status ohm_ctx_synchronize(ohm_ctx *ctx);
 /* The CUDA stream (cudaStream_t) the context launches on. */
 void *ohm_ctx_stream(ohm_ctx *ctx);
+/* Where the Krylov solves of this context's single-system solver keep their
+ * working set (no counterpart in the reference, whose BiCGSTAB is a sequence
+ * of dispatches; a tuning and testing switch):
+ *   OHM_KRYLOV_LAYOUT_AUTO     each block's CSR slice and Krylov state in
+ *                              shared memory where the slice fits, else in
+ *                              global memory (default)
+ *   OHM_KRYLOV_LAYOUT_GLOBAL   global memory for every block: the path of
+ *                              systems too large for the slices, at any size
+ * The two give the same iterates bit for bit.  Batches, transients and the
+ * allocation-free solve keep their own choice. */
+#define OHM_KRYLOV_LAYOUT_AUTO 0
+#define OHM_KRYLOV_LAYOUT_GLOBAL 1
+ohm_status ohm_ctx_set_krylov_layout(ohm_ctx *ctx, int32_t layout);
 
 /* ---- SolverBackend (src/solver/backend.rs:51-96) ------------------------ */
 ohm_status ohm_buf_create(ohm_ctx *ctx, int64_t n, ohm_buf **out);            /* new_buffer (zeroed) */

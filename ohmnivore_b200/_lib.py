@@ -19,6 +19,7 @@ OK, ERR_SOLVE, ERR_NEWTON_NOT_CONVERGED, ERR_NEWTON_NUMERICAL, ERR_COMPILE, ERR_
 PREC_FP64, PREC_MIXED = 0, 1
 PRECOND_AUTO, PRECOND_JACOBI, PRECOND_ISAI1, PRECOND_NONE = 0, 1, 2, 3
 CONT_ON, CONT_TEST_PSEUDO = 1, 2   # ohm_newton_params.continuation bits
+KRYLOV_LAYOUT_AUTO, KRYLOV_LAYOUT_GLOBAL = 0, 1   # ohm_ctx_set_krylov_layout
 
 
 class KrylovParams(C.Structure):
@@ -115,6 +116,7 @@ SIGNATURES = {
     "ohm_ctx_destroy": (C.c_int, [_vp]),
     "ohm_ctx_synchronize": (C.c_int, [_vp]),
     "ohm_ctx_stream": (_vp, [_vp]),
+    "ohm_ctx_set_krylov_layout": (C.c_int, [_vp, C.c_int32]),
     "ohm_buf_create": (C.c_int, [_vp, _i64, C.POINTER(_vp)]),
     "ohm_buf_destroy": (C.c_int, [_vp]),
     "ohm_buf_upload": (C.c_int, [_vp, _vp, _dp, _i64]),

@@ -133,6 +133,14 @@ extern "C" ohm_status ohm_ctx_synchronize(ohm_ctx *c) {
 
 extern "C" void *ohm_ctx_stream(ohm_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
+extern "C" ohm_status ohm_ctx_set_krylov_layout(ohm_ctx *c, int32_t layout) {
+    if (!c) return fail(OHM_ERR_INVALID_ARG, "context is null");
+    if (layout != OHM_KRYLOV_LAYOUT_AUTO && layout != OHM_KRYLOV_LAYOUT_GLOBAL)
+        return fail(OHM_ERR_INVALID_ARG, "unknown Krylov layout %d", (int)layout);
+    c->krylov_layout = layout;
+    return OHM_OK;
+}
+
 // ------------------------------------------------------------ launch logic --
 using KernelFn = void (*)(KernelArgs);
 
@@ -194,7 +202,8 @@ ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t n
     if (t.max_grid > 0) cap = std::min<int64_t>(cap, t.max_grid);
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
     // one block per SM either way: a block is 1024 threads at the register cap
-    a.smem_bytes = ohm_krylov_smem_bytes((const void *)fn, a.n, nnz - a.nnz_long, grid);
+    a.smem_bytes = t.krylov_layout != OHM_KRYLOV_LAYOUT_GLOBAL
+                       ? ohm_krylov_smem_bytes((const void *)fn, a.n, nnz - a.nnz_long, grid) : 0;
     if (a.smem_bytes > 0) {
         int fit = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kBlock, a.smem_bytes));
@@ -214,7 +223,7 @@ ohm_status ohm_launch_persistent(const LaunchTarget &t, KernelArgs &a, int64_t n
 }
 
 static LaunchTarget ctx_target(ohm_ctx *c) {
-    return LaunchTarget{c->num_sms, c->stream, c->sync_words, c->info_dev, c->info_host, 0};
+    return LaunchTarget{c->num_sms, c->stream, c->sync_words, c->info_dev, c->info_host, 0, c->krylov_layout};
 }
 
 static ohm_status launch_solver(ohm_ctx *c, KernelArgs &a, int64_t nnz, int *launches) {

@@ -32,6 +32,7 @@ struct ohm_ctx {
     DeviceInfo *info_dev = nullptr;
     DeviceInfo *info_host = nullptr;      // pinned
     double *dot_scratch = nullptr;        // for ohm_dot
+    int krylov_layout = 0;                    // OHM_KRYLOV_LAYOUT_*
     // Objects created on this context (plans, buffers, matrices).  Destroying
     // the context while some are alive defers the release to the last one.
     int live_objects = 0;
@@ -46,6 +47,7 @@ struct LaunchTarget {
     ohm::DeviceInfo *info_dev;
     ohm::DeviceInfo *info_host;      // host copy target (pinned or not)
     int max_grid;                    // 0: no cap beyond the co-residency limit
+    int krylov_layout;               // OHM_KRYLOV_LAYOUT_* (0 when not given)
 };
 ohm_status ohm_launch_persistent(const LaunchTarget &t, ohm::KernelArgs &a, int64_t nnz, int *launches);
 ohm_status ohm_finish_persistent(const LaunchTarget &t, ohm_solve_info *info, int launches);

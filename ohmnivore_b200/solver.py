@@ -172,6 +172,15 @@ class Context:
         if st:
             _raise(st)
 
+    def set_krylov_layout(self, layout: int):
+        """Where single-system Krylov solves keep their working set:
+        ``_lib.KRYLOV_LAYOUT_AUTO`` (each block's slice in shared memory where
+        it fits, else global memory) or ``KRYLOV_LAYOUT_GLOBAL`` (global
+        memory for every block, the path of large systems, at any size)."""
+        st = self.lib.ohm_ctx_set_krylov_layout(self._h, int(layout))
+        if st:
+            _raise(st)
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.ohm_ctx_destroy(self._h)
