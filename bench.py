@@ -524,7 +524,10 @@ def batch_section(args, S, ctx, stream, barrier, world, rank, local_rank):
            "value": args.batch / (ms * 1e-3), "unit": "solves/s", "ms": ms,
            "scaling": "strong: the instances are sharded over the GPUs (LPT), one batch launch per GPU"
                       if world > 1 else "1 GPU",
-           "precision": "FP64", "kernel_launches": 1, "failed_instances": int(np.count_nonzero(status_all != 0)),
+           "precision": "FP64", "kernel_launches": info["kernel_launches"],
+           "split": "circuits whose one-block solve would outlast the rest run alone on the whole GPU first "
+                    "(ohm_batch_set_split); kernel_launches counts those solves and the batch launch",
+           "failed_instances": int(np.count_nonzero(status_all != 0)),
            "continuation_instances": int(cont[0].item()),
            "krylov_iterations": info["krylov_iterations"], "autotune": choice,
            "autotune_s": tune_s, "host_setup_s": setup_s, "device_compile_s": compile_s, "clocks": clk.summary()}

@@ -538,6 +538,17 @@ ohm_status ohm_batch_autotune(ohm_batch *batch, const ohm_newton_params *params,
 /* Choose the kernel variant directly (same choices as the autotuner). */
 ohm_status ohm_batch_set_kernel(ohm_batch *batch, int32_t lanes_per_row, int32_t threads_per_block,
                                 int32_t blocks_per_sm);
+/* Split of each ohm_batch_newton_device call (on = 1, the default; 0 = every
+ * instance in the batch kernel).  With few instances of mixed sizes one block
+ * on the largest circuit would set the call's time while the other SMs idle,
+ * so a circuit whose one-block solve is estimated (rows^1.5) to outlast the
+ * rest of the batch spread over the resident blocks, and that has at least
+ * 2,048 rows (below that one block beats the whole grid), is solved first,
+ * alone, by the single-system persistent solver on the whole GPU; the batch
+ * kernel then takes the rest.  summary's
+ * kernel_launches counts both.  Large batches of similar sizes split nothing.
+ * No counterpart in the reference (its batch is many newton_solve calls). */
+ohm_status ohm_batch_set_split(ohm_batch *batch, int32_t on);
 
 /* ---------------------------------------------------------------- compile --
  * Device-side MNA compile of compile (src/compiler.rs:194-754): node

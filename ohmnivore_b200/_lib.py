@@ -117,6 +117,7 @@ SIGNATURES = {
     "ohm_ctx_synchronize": (C.c_int, [_vp]),
     "ohm_ctx_stream": (_vp, [_vp]),
     "ohm_ctx_set_krylov_layout": (C.c_int, [_vp, C.c_int32]),
+    "ohm_batch_set_split": (C.c_int, [_vp, C.c_int32]),
     "ohm_buf_create": (C.c_int, [_vp, _i64, C.POINTER(_vp)]),
     "ohm_buf_destroy": (C.c_int, [_vp]),
     "ohm_buf_upload": (C.c_int, [_vp, _vp, _dp, _i64]),

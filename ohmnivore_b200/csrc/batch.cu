@@ -29,6 +29,12 @@ struct ohm_batch {
     std::vector<DeviceInfo> host_infos;
     DeviceInfo *infos = nullptr;
     unsigned int *queue = nullptr;
+    // Host copies of the offset tables and of the largest-first order, for
+    // instances solved one at a time by the whole GPU (ohm_batch_set_split).
+    std::vector<InstanceOffsets> h_offsets;
+    std::vector<int32_t> h_order;
+    double *team_partials = nullptr;   // reduction partials of those solves
+    int split = 1;
 
     template <typename T>
     cudaError_t put(T **dst, const T *src, size_t count) {
@@ -198,6 +204,7 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     PUT(i64, rid_off.data(), n_inst + 1); b->args.rid_off = i64;
     PUT(i32, order.data(), n_inst); b->args.order = i32; b->order = i32;
     ZERO(b->sample, n_inst);
+    ZERO(b->team_partials, 8 * (size_t)c->num_sms * 8);
     ZERO(b->infos, n_inst);
     ZERO(b->queue, 4);
 #undef PUT
@@ -213,6 +220,17 @@ extern "C" ohm_status ohm_batch_create(ohm_ctx *c, int64_t n_inst, const int64_t
     b->args.infos = b->infos;
     b->args.queue = b->queue;
     b->host_infos.resize(n_inst);
+    b->h_order = order;
+    b->h_offsets.resize(n_inst);
+    for (int64_t i = 0; i < n_inst; ++i) {
+        InstanceOffsets &o = b->h_offsets[i];
+        o.ro = row_off[i]; o.ro1 = row_off[i + 1]; o.no = nnz_off[i]; o.no1 = nnz_off[i + 1];
+        o.dq = diode_off[i]; o.dq1 = diode_off[i + 1]; o.qq = bjt_off[i]; o.qq1 = bjt_off[i + 1];
+        o.mq = mosfet_off[i]; o.mq1 = mosfet_off[i + 1];
+        o.ms = ms_off[i]; o.ms1 = ms_off[i + 1]; o.mid = mid_off[i];
+        o.rs = rs_off[i]; o.rs1 = rs_off[i + 1]; o.rid = rid_off[i];
+        o.n_nodes = n_nodes ? n_nodes[i] : 0;
+    }
     ohm_ctx_retain(c);
     *out = b;
     return OHM_OK;
@@ -282,6 +300,70 @@ static ohm_status launch_batch(ohm_batch *b, BatchArgs B, int lpr, int shape, in
     return OHM_OK;
 }
 
+// Split of one call: a circuit whose solve by one block would outlast the
+// rest of the batch goes to the whole GPU instead.  A one-block solve is
+// estimated as rows^1.5 (Krylov iterations grow about as the square root
+// of a mesh's size); in largest-first order, circuits move while the next
+// one's estimate exceeds the ideal length of the rest (the sum of their
+// estimates over the resident blocks) and it has at least 2,048 rows (below
+// that one block beats the grid, whose barriers cost microseconds each).
+constexpr int64_t kSplitMinRows = 2048;
+
+static void split_instances(const ohm_batch *b, int lpr, int shape, std::vector<int32_t> &team,
+                            std::vector<int32_t> &rest) {
+    team.clear();
+    rest.clear();
+    int per_sm = 0;
+    const BatchFn fn = batch_kernel(lpr, shape);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchShapes[shape].block, 0) != cudaSuccess)
+        per_sm = 1;
+    const double blocks = (double)std::max(per_sm, 1) * (double)b->ctx->num_sms;
+    auto est = [&](int32_t i) {
+        const double n = (double)(b->h_offsets[i].ro1 - b->h_offsets[i].ro);
+        return n * std::sqrt(n);
+    };
+    double total = 0.0;
+    for (int32_t i : b->h_order) total += est(i);
+    size_t k = 0;
+    if (b->split) {
+        for (; k < b->h_order.size(); ++k) {
+            const int32_t i = b->h_order[k];
+            const double t = est(i);
+            if (b->h_offsets[i].ro1 - b->h_offsets[i].ro < kSplitMinRows || t <= (total - t) / blocks) break;
+            team.push_back(i);
+            total -= t;
+        }
+    }
+    rest.assign(b->h_order.begin() + (ptrdiff_t)k, b->h_order.end());
+}
+
+// Solves instance i alone with the single-system persistent solver over the
+// batch's packed arrays; its status lands in the batch's per-instance info.
+static ohm_status solve_instance_whole_gpu(ohm_batch *b, const BatchArgs &B, int32_t i, int *launches) {
+    ohm_ctx *c = b->ctx;
+    KernelArgs a;
+    instance_args(B, i, b->h_offsets[i], a);
+    a.partials = b->team_partials;
+    const LaunchTarget t{c->num_sms, c->stream, c->sync_words, c->info_dev, c->info_host, 0, c->krylov_layout};
+    ohm_status st = ohm_launch_persistent(t, a, a.nnz, launches);
+    if (st != OHM_OK) return st;
+    CUDA_TRY(cudaMemcpyAsync(b->infos + i, c->info_dev, sizeof(DeviceInfo), cudaMemcpyDeviceToDevice, c->stream));
+    unsigned int words[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(words, c->sync_words, sizeof words, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (words[2] != 0)
+        return ohm_fail(OHM_ERR_TIMEOUT, "instance %d: a device barrier wait gave up (error word %u)", (int)i,
+                        words[2]);
+    return OHM_OK;
+}
+
+extern "C" ohm_status ohm_batch_set_split(ohm_batch *b, int32_t on) {
+    if (!b) return ohm_fail(OHM_ERR_INVALID_ARG, "batch is null");
+    if (on != 0 && on != 1) return ohm_fail(OHM_ERR_INVALID_ARG, "split must be 0 or 1");
+    b->split = on;
+    return OHM_OK;
+}
+
 extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const ohm_newton_params *np,
                                               ohm_solve_info *summary) {
     BatchArgs B;
@@ -292,8 +374,24 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
     if (np->initial_guess)
         CUDA_TRY(cudaMemcpyAsync(x_dev, np->initial_guess, b->rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemsetAsync(b->infos, 0, b->n_inst * sizeof(DeviceInfo), c->stream));
-    st = launch_batch(b, B, b->lpr, b->shape, (int)b->n_inst, b->order);
-    if (st != OHM_OK) return st;
+    std::vector<int32_t> team, rest;
+    split_instances(b, b->lpr, b->shape, team, rest);
+    int launches = 0;
+    for (int32_t i : team) {
+        st = solve_instance_whole_gpu(b, B, i, &launches);
+        if (st != OHM_OK) return st;
+    }
+    if (!rest.empty()) {
+        const int32_t *order = b->order;
+        if (!team.empty()) {   // the rest of the largest-first order (the autotune sample array is free here)
+            CUDA_TRY(cudaMemcpyAsync(b->sample, rest.data(), rest.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                     c->stream));
+            order = b->sample;
+        }
+        st = launch_batch(b, B, b->lpr, b->shape, (int)rest.size(), order);
+        if (st != OHM_OK) return st;
+        ++launches;
+    }
     CUDA_TRY(cudaMemcpyAsync(b->host_infos.data(), b->infos, b->n_inst * sizeof(DeviceInfo), cudaMemcpyDeviceToHost,
                              c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -316,7 +414,7 @@ extern "C" ohm_status ohm_batch_newton_device(ohm_batch *b, double *x_dev, const
         summary->krylov_iterations = kit;
         summary->fp64_fallbacks = (int32_t)fb;
         summary->krylov_restarts = (int32_t)rs;
-        summary->kernel_launches = 1;
+        summary->kernel_launches = launches;
         summary->status = worst < 0 ? OHM_OK : b->host_infos[worst].status;
         summary->error_iteration = (int32_t)worst;
         summary->continuation_steps = (int32_t)std::min<int64_t>(csteps, 0x7fffffff);

@@ -24,7 +24,70 @@ struct BatchArgs {
 };
 
 template <typename P>
-__device__ __forceinline__ P *offset(P *p, int64_t k) { return p ? p + k : p; }
+__host__ __device__ inline P *offset(P *p, int64_t k) { return p ? p + k : p; }
+
+// Where instance i sits in the packed arrays (read from BatchArgs' device
+// tables by the batch kernel, from host copies by the whole-GPU path).
+struct InstanceOffsets {
+    int64_t ro, ro1, no, no1, dq, dq1, qq, qq1, mq, mq1, ms, ms1, mid, rs, rs1, rid;
+    int n_nodes;
+};
+
+// Kernel arguments of instance i: B.base with every per-row, per-nonzero and
+// per-device pointer moved to the instance's slice.
+__host__ __device__ inline void instance_args(const BatchArgs &B, int i, const InstanceOffsets &o, KernelArgs &a) {
+    const int64_t ro = o.ro, no = o.no;
+    const int64_t dq = o.dq, qq = o.qq, mq = o.mq;
+    a = B.base;
+    a.n = (int)(o.ro1 - ro);
+    a.nnz = (int)(o.no1 - no);
+    a.row_ptr = B.base.row_ptr + ro + i;               // n_i + 1 local row pointers
+    a.col = B.base.col + no;
+    a.vals64 = B.base.vals64 + no;
+    a.vals32 = offset(B.base.vals32, no);
+    a.base_vals = B.base.base_vals + no;
+    a.base_b = B.base.base_b + ro;
+    a.b = B.base.b + ro;
+    a.x = B.base.x + ro;
+    a.x_prev = B.base.x_prev + ro;
+    a.r64 = B.base.r64 + ro;
+    a.dx = B.base.dx + ro;
+    a.partner = B.base.partner + ro;
+    a.diag_slot = B.base.diag_slot + ro;
+    a.off_slot = B.base.off_slot + ro;
+    a.rowflag = offset(B.base.rowflag, ro);
+    a.pc_part = (double *)B.base.pc_part + ro;
+    a.rec0 = (double *)B.base.rec0 + 4 * ro;
+    a.rec1 = (double *)B.base.rec1 + 4 * ro;
+    a.rhat = (double *)B.base.rhat + ro;
+    a.s = (double *)B.base.s + ro;
+    a.t = (double *)B.base.t + ro;
+    a.phat = (double *)B.base.phat + ro;
+    a.shat = (double *)B.base.shat + ro;
+    a.d = (double *)B.base.d + ro;
+    a.nd = (int)(o.dq1 - dq);
+    a.nq = (int)(o.qq1 - qq);
+    a.nm = (int)(o.mq1 - mq);
+    a.diodes = B.base.diodes + dq;
+    a.bjts = B.base.bjts + qq;
+    a.mosfets = B.base.mosfets + mq;
+    a.bjt_vaf = offset(B.base.bjt_vaf, qq);
+    a.mstamp = B.base.mstamp + 4 * dq + 9 * qq + 6 * mq;
+    a.rstamp = B.base.rstamp + 2 * dq + 3 * qq + 2 * mq;
+    a.n_mslots = (int)(o.ms1 - o.ms);
+    a.mslot = B.base.mslot + o.ms;
+    a.mslot_ptr = B.base.mslot_ptr + o.ms + i;
+    a.mslot_ids = B.base.mslot_ids + o.mid;
+    a.n_rrows = (int)(o.rs1 - o.rs);
+    a.rrow = B.base.rrow + o.rs;
+    a.rrow_ptr = B.base.rrow_ptr + o.rs + i;
+    a.rrow_ids = B.base.rrow_ids + o.rid;
+    a.node_scale = (unsigned long long *)(B.node_scale_base + ro);
+    a.trace = nullptr;
+    a.n_nodes = o.n_nodes;
+    a.stampflag = B.stampflag + ro;
+    a.x_good = B.x_good + ro;
+}
 
 template <int LPR, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_solver(BatchArgs B) {
@@ -37,57 +100,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_solver(BatchArgs B) {
         __syncthreads();
         if (q >= B.n_inst) return;
         const int i = B.order[q];
-        const int64_t ro = B.row_off[i], no = B.nnz_off[i];
-        const int64_t dq = B.d_off[i], qq = B.q_off[i], mq = B.m_off[i];
-        KernelArgs a = B.base;
-        a.n = (int)(B.row_off[i + 1] - ro);
-        a.nnz = (int)(B.nnz_off[i + 1] - no);
-        a.row_ptr = B.base.row_ptr + ro + i;               // n_i + 1 local row pointers
-        a.col = B.base.col + no;
-        a.vals64 = B.base.vals64 + no;
-        a.vals32 = offset(B.base.vals32, no);
-        a.base_vals = B.base.base_vals + no;
-        a.base_b = B.base.base_b + ro;
-        a.b = B.base.b + ro;
-        a.x = B.base.x + ro;
-        a.x_prev = B.base.x_prev + ro;
-        a.r64 = B.base.r64 + ro;
-        a.dx = B.base.dx + ro;
-        a.partner = B.base.partner + ro;
-        a.diag_slot = B.base.diag_slot + ro;
-        a.off_slot = B.base.off_slot + ro;
-        a.rowflag = offset(B.base.rowflag, ro);
-        a.pc_part = (double *)B.base.pc_part + ro;
-        a.rec0 = (double *)B.base.rec0 + 4 * ro;
-        a.rec1 = (double *)B.base.rec1 + 4 * ro;
-        a.rhat = (double *)B.base.rhat + ro;
-        a.s = (double *)B.base.s + ro;
-        a.t = (double *)B.base.t + ro;
-        a.phat = (double *)B.base.phat + ro;
-        a.shat = (double *)B.base.shat + ro;
-        a.d = (double *)B.base.d + ro;
-        a.nd = (int)(B.d_off[i + 1] - dq);
-        a.nq = (int)(B.q_off[i + 1] - qq);
-        a.nm = (int)(B.m_off[i + 1] - mq);
-        a.diodes = B.base.diodes + dq;
-        a.bjts = B.base.bjts + qq;
-        a.mosfets = B.base.mosfets + mq;
-        a.bjt_vaf = offset(B.base.bjt_vaf, qq);
-        a.mstamp = B.base.mstamp + 4 * dq + 9 * qq + 6 * mq;
-        a.rstamp = B.base.rstamp + 2 * dq + 3 * qq + 2 * mq;
-        a.n_mslots = (int)(B.ms_off[i + 1] - B.ms_off[i]);
-        a.mslot = B.base.mslot + B.ms_off[i];
-        a.mslot_ptr = B.base.mslot_ptr + B.ms_off[i] + i;
-        a.mslot_ids = B.base.mslot_ids + B.mid_off[i];
-        a.n_rrows = (int)(B.rs_off[i + 1] - B.rs_off[i]);
-        a.rrow = B.base.rrow + B.rs_off[i];
-        a.rrow_ptr = B.base.rrow_ptr + B.rs_off[i] + i;
-        a.rrow_ids = B.base.rrow_ids + B.rid_off[i];
-        a.node_scale = (unsigned long long *)(B.node_scale_base + ro);
-        a.trace = nullptr;
-        a.n_nodes = B.n_nodes ? B.n_nodes[i] : 0;
-        a.stampflag = B.stampflag + ro;
-        a.x_good = B.x_good + ro;
+        InstanceOffsets o;
+        o.ro = B.row_off[i]; o.ro1 = B.row_off[i + 1]; o.no = B.nnz_off[i]; o.no1 = B.nnz_off[i + 1];
+        o.dq = B.d_off[i]; o.dq1 = B.d_off[i + 1]; o.qq = B.q_off[i]; o.qq1 = B.q_off[i + 1];
+        o.mq = B.m_off[i]; o.mq1 = B.m_off[i + 1];
+        o.ms = B.ms_off[i]; o.ms1 = B.ms_off[i + 1]; o.mid = B.mid_off[i];
+        o.rs = B.rs_off[i]; o.rs1 = B.rs_off[i + 1]; o.rid = B.rid_off[i];
+        o.n_nodes = B.n_nodes ? B.n_nodes[i] : 0;
+        KernelArgs a;
+        instance_args(B, i, o, a);
         BlockTeam g;
         g.r0 = 0;
         g.r1 = a.n;

@@ -482,6 +482,13 @@ class NewtonBatch:
         if st:
             _raise(st)
 
+    def set_split(self, on: bool):
+        """Solve the circuits that would set a call's time alone on the whole
+        GPU before the batch kernel takes the rest (default on)."""
+        st = self.ctx.lib.ohm_batch_set_split(self._h, 1 if on else 0)
+        if st:
+            _raise(st)
+
     def instance_info(self):
         arr = (_lib.SolveInfo * self.n_instances)()
         st = self.ctx.lib.ohm_batch_instance_info(self._h, arr, self.n_instances)

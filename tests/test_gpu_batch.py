@@ -183,3 +183,27 @@ def test_batch_autotune(ctx):
         batch.close()
     assert info["status"] == 0
     _check_all(systems, batch.split(x))
+
+
+def test_batch_split_solves_large_circuit_on_whole_gpu(ctx):
+    """One 3,600-row diode mesh among small Monte Carlo circuits: its
+    one-block solve would outlast the rest of the batch, so the split solves
+    it alone on the whole GPU first (two launches); the results match the
+    oracle and the unsplit batch."""
+    cs = [ck.diode_mesh(60, 60, seed=2)] + ck.monte_carlo_batch(24, seed=3, n_lo=50, n_hi=600, vaf=np.inf)[:7]
+    systems = [mna.compile_circuit(c) for c in cs]
+    assert systems[0].size >= 2048
+    batch = S.NewtonBatch(systems, ctx)
+    try:
+        x_split, info_split = _solve(batch, params=_params(0))
+        per = batch.instance_info()
+        batch.set_split(False)
+        x_one, info_one = _solve(batch, params=_params(0))
+    finally:
+        batch.close()
+    assert info_split["kernel_launches"] == 2
+    assert info_one["kernel_launches"] == 1
+    assert all(p["status"] == 0 and p["iterations"] >= 1 for p in per)
+    assert info_split["iterations"] == max(p["iterations"] for p in per)
+    _check_all(systems, batch.split(x_split))
+    assert _rel(x_split, x_one) < 1e-10
