@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -41,6 +42,71 @@ struct AcArgs {
     double2 *work;                     // kAcVecs * n per frequency point
     AcDev *info;
     unsigned int *queue;
+    // Team mode (fewer points than resident blocks): block b works on point
+    // blk_point[b] as member blk_member[b] of point_team[q] blocks, with a
+    // per-point barrier counter and reduction partials [2][4][kAcMaxTeam].
+    int team_mode;
+    const int32_t *blk_point, *blk_member, *point_team;
+    unsigned long long *team_count;
+    double *team_part;
+    int *team_error;
+};
+
+constexpr int kAcMaxTeam = 8;
+
+// The blocks solving one frequency point.  A one-block team (TEAM false, the
+// queue mode) synchronises and reduces within the block; a team of T blocks
+// splits the rows evenly and meets at a bounded barrier on the point's
+// arrival counter, its dot products summed from per-member partials in
+// member order (identical in every member).
+template <bool TEAM>
+struct AcTeam {
+    int T, m, r0, r1;
+    unsigned long long *count;
+    unsigned long long epoch;
+    double *part;
+    int red;
+    int *error;
+    double *smem;
+
+    __device__ __forceinline__ bool sync() {
+        if constexpr (!TEAM) { __syncthreads(); return true; }
+        __shared__ int s_ok;
+        epoch += (unsigned long long)T;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            red_release_add_u64(count, 1ull);
+            int ok = 1;
+            uint32_t spins = 0;
+            while (ld_acquire_u64(count) < epoch) {
+                if (++spins > kBarrierSpinLimit || *(volatile int *)error != 0) {
+                    atomicCAS(error, 0, kStatusTimeout);
+                    ok = 0;
+                    break;
+                }
+                if (spins > kTightSpins) __nanosleep(64);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
+    template <int NV>
+    __device__ __forceinline__ bool sum(double (&v)[NV]) {
+        block_sum<NV>(v, smem);
+        if constexpr (!TEAM) return true;
+        double *p = part + (size_t)(red & 1) * 4 * kAcMaxTeam;
+        ++red;
+        if (threadIdx.x == 0)
+            for (int k = 0; k < NV; ++k) p[k * kAcMaxTeam + m] = v[k];
+        if (!sync()) return false;
+        for (int k = 0; k < NV; ++k) {
+            double x = 0.0;
+            for (int j = 0; j < T; ++j) x += __ldcg(p + k * kAcMaxTeam + j);
+            v[k] = x;
+        }
+        return true;
+    }
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -61,13 +127,13 @@ __device__ __forceinline__ double2 cval(const AcArgs &A, uint32_t k, double w) {
     return make_double2(A.g[k], A.c ? w * A.c[k] : 0.0);
 }
 
-// y_i = sum_k A(f)_ik x_k for every row, LPR lanes per row; f(i, y).
+// y_i = sum_k A(f)_ik x_k for rows [r0, r1), LPR lanes per row; f(i, y).
 template <int LPR, typename F>
-__device__ __forceinline__ void cspmv(const AcArgs &A, double w, const double2 *x, F f) {
+__device__ __forceinline__ void cspmv(const AcArgs &A, double w, const double2 *x, int r0, int r1, F f) {
     const int lane = threadIdx.x % LPR, group = threadIdx.x / LPR, ngroups = blockDim.x / LPR;
-    for (int base = 0; base < A.n; base += ngroups) {
+    for (int base = r0; base < r1; base += ngroups) {
         const int i = base + group;
-        const bool ok = i < A.n;
+        const bool ok = i < r1;
         const uint32_t b = ok ? A.rp[i] : 0u, e = ok ? A.rp[i + 1] : 0u;
         uint32_t len = e - b;
 #pragma unroll
@@ -86,17 +152,12 @@ __device__ __forceinline__ void cspmv(const AcArgs &A, double w, const double2 *
     }
 }
 
-template <int LPR, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
-    __shared__ double smem[32 * 4];
-    __shared__ int s_q;
-    const int n = A.n;
-    for (;;) {
-        if (threadIdx.x == 0) s_q = (int)atomicAdd(A.queue, 1u);
-        __syncthreads();
-        const int q = s_q;
-        __syncthreads();
-        if (q >= A.n_freq) return;
+// One frequency point solved by team g (rows [g.r0, g.r1) of this block).
+// Returns false when a team barrier gave up.
+template <int LPR, bool TEAM>
+__device__ bool ac_point(const AcArgs &A, int q, AcTeam<TEAM> &g) {
+    const int n = A.n, r0 = g.r0, r1 = g.r1;
+    {
         const double w = A.omega[q];
         double2 *W = A.work + (size_t)q * kAcVecs * n;
         double2 *x = W, *r = W + n, *rh = W + 2 * (size_t)n, *p = W + 3 * (size_t)n, *v = W + 4 * (size_t)n;
@@ -105,7 +166,7 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
 
         // preconditioner coefficients for this frequency, and the start vectors
         double acc0[1] = {0.0};
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
             double2 cs = make_double2(0.0, 0.0), cp = make_double2(0.0, 0.0);
             const uint32_t ds = A.diag_slot[i];
             const double2 aii = ds == kSentinel ? make_double2(0.0, 0.0) : cval(A, ds, w);
@@ -137,7 +198,7 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
             v[i] = make_double2(0.0, 0.0);
             acc0[0] += cabs2(bi);
         }
-        block_sum<1>(acc0, smem);
+        if (!g.sum<1>(acc0)) return false;
         const double bnorm = sqrt(acc0[0]);
         int code = kKrylovRunning, it = 0, restarts = 0;
         double rnorm = bnorm;
@@ -148,87 +209,91 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
             double2 rho = make_double2(1.0, 0.0), alpha = rho, omega = rho;
             double2 rho_new = make_double2(acc0[0], 0.0);
             double rr = acc0[0], rh2 = acc0[0];
-            auto restart = [&]() {
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            auto restart = [&]() -> bool {
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                     rh[i] = r[i];
                     p[i] = make_double2(0.0, 0.0);
                     v[i] = make_double2(0.0, 0.0);
                 }
-                __syncthreads();
+                if (!g.sync()) return false;
                 rho = make_double2(1.0, 0.0);
                 alpha = rho;
                 omega = rho;
                 rho_new = make_double2(rr, 0.0);
                 rh2 = rr;
                 ++restarts;
+                return true;
             };
             for (; it < A.max_it; ++it) {
                 if (!(sqrt(cabs2(rho_new)) >= kBreakdownRel * sqrt(rh2 * rr))) {
-                    if (restarts < A.max_restarts && rr > 0.0) restart();
+                    if (restarts < A.max_restarts && rr > 0.0) { if (!restart()) return false; }
                     else { code = kKrylovBreakRho; break; }
                 }
                 const double2 beta = cmul(cdiv(rho_new, rho), cdiv(alpha, omega));
                 rho = rho_new;
-                for (int i = threadIdx.x; i < n; i += blockDim.x)
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
                     p[i] = cadd(cmul(csub(p[i], cmul(omega, v[i])), beta), r[i]);
-                __syncthreads();
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                if (!g.sync()) return false;
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                     double2 z = cmul(ms[i], p[i]);
                     const int pi = A.partner[i];
                     if (pi >= 0) z = cadd(z, cmul(mp[i], p[pi]));
                     ph[i] = z;
                 }
-                __syncthreads();
+                if (!g.sync()) return false;
                 double a1[4] = {0.0, 0.0, 0.0, 0.0};     // r_hat^H v, ||v||^2
-                cspmv<LPR>(A, w, ph, [&](int i, double2 y) {
+                cspmv<LPR>(A, w, ph, r0, r1, [&](int i, double2 y) {
                     v[i] = y;
                     const double2 d = cdotc(rh[i], y);
                     a1[0] += d.x;
                     a1[1] += d.y;
                     a1[2] += cabs2(y);
                 });
-                block_sum<4>(a1, smem);
+                if (!g.sum<4>(a1)) return false;
                 const double2 rhv = make_double2(a1[0], a1[1]);
                 if (!(sqrt(cabs2(rhv)) >= kBreakdownRel * sqrt(rh2 * a1[2]))) {
-                    if (restarts < A.max_restarts && rr > 0.0) { restart(); continue; }
+                    if (restarts < A.max_restarts && rr > 0.0) {
+                        if (!restart()) return false;
+                        continue;
+                    }
                     code = kKrylovBreakRv;
                     break;
                 }
                 alpha = cdiv(rho, rhv);
                 double a2[1] = {0.0};
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                     const double2 si = csub(r[i], cmul(alpha, v[i]));
                     s[i] = si;
                     a2[0] += cabs2(si);
                 }
-                block_sum<1>(a2, smem);
+                if (!g.sum<1>(a2)) return false;
                 if (sqrt(a2[0]) < abs_tol) {                     // gpu.rs:646-650
-                    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = cadd(x[i], cmul(alpha, ph[i]));
+                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) x[i] = cadd(x[i], cmul(alpha, ph[i]));
                     rnorm = sqrt(a2[0]);
                     code = kKrylovConverged;
                     ++it;
                     break;
                 }
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                     double2 z = cmul(ms[i], s[i]);
                     const int pi = A.partner[i];
                     if (pi >= 0) z = cadd(z, cmul(mp[i], s[pi]));
                     sh[i] = z;
                 }
-                __syncthreads();
+                if (!g.sync()) return false;
                 double a3[3] = {0.0, 0.0, 0.0};          // t^H s, t^H t
-                cspmv<LPR>(A, w, sh, [&](int i, double2 y) {
+                cspmv<LPR>(A, w, sh, r0, r1, [&](int i, double2 y) {
                     t[i] = y;
                     const double2 d = cdotc(y, s[i]);
                     a3[0] += d.x;
                     a3[1] += d.y;
                     a3[2] += cabs2(y);
                 });
-                block_sum<3>(a3, smem);
+                if (!g.sum<3>(a3)) return false;
                 if (!(a3[2] > 0.0)) { code = kKrylovBreakTt; break; }
                 omega = cdiv(make_double2(a3[0], a3[1]), make_double2(a3[2], 0.0));
                 double a4[3] = {0.0, 0.0, 0.0};          // r_hat^H r, ||r||^2
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
                     x[i] = cadd(cadd(x[i], cmul(alpha, ph[i])), cmul(omega, sh[i]));
                     const double2 ri = csub(s[i], cmul(omega, t[i]));
                     r[i] = ri;
@@ -237,7 +302,7 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
                     a4[1] += d.y;
                     a4[2] += cabs2(ri);
                 }
-                block_sum<3>(a4, smem);
+                if (!g.sum<3>(a4)) return false;
                 rho_new = make_double2(a4[0], a4[1]);
                 rr = a4[2];
                 rnorm = sqrt(rr);
@@ -248,7 +313,7 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
             if (code == kKrylovRunning) code = kKrylovMaxIter;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (g.m == 0 && threadIdx.x == 0) {
             AcDev &d = A.info[q];
             d.code = code;
             d.iterations = it;
@@ -257,6 +322,53 @@ __global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
             d.bnorm = bnorm;
         }
         __syncthreads();
+    }
+    return true;
+}
+
+// Team mode (cooperative launch, fewer points than resident blocks): block
+// b solves point blk_point[b] with the other members of its team.
+template <int LPR>
+__global__ void __launch_bounds__(kAcWideBlock) ac_team_kernel(AcArgs A) {
+    __shared__ double smem[32 * 4];
+    AcTeam<true> g;
+    g.smem = smem;
+    g.epoch = 0;
+    g.red = 0;
+    const int q = A.blk_point[blockIdx.x];
+    g.T = A.point_team[q];
+    g.m = A.blk_member[blockIdx.x];
+    g.r0 = (int)(((long long)A.n * g.m) / g.T);
+    g.r1 = (int)(((long long)A.n * (g.m + 1)) / g.T);
+    g.count = A.team_count + q;
+    g.part = A.team_part + (size_t)q * 8 * kAcMaxTeam;
+    g.error = A.team_error;
+    ac_point<LPR, true>(A, q, g);
+}
+
+// Queue mode: each block takes points from the queue and solves each alone.
+template <int LPR, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ac_sweep_kernel(AcArgs A) {
+    __shared__ double smem[32 * 4];
+    __shared__ int s_q;
+    AcTeam<false> g;
+    g.smem = smem;
+    g.epoch = 0;
+    g.red = 0;
+    g.T = 1;
+    g.m = 0;
+    g.r0 = 0;
+    g.r1 = A.n;
+    g.count = nullptr;
+    g.part = nullptr;
+    g.error = nullptr;
+    for (;;) {
+        if (threadIdx.x == 0) s_q = (int)atomicAdd(A.queue, 1u);
+        __syncthreads();
+        const int q = s_q;
+        __syncthreads();
+        if (q >= A.n_freq) return;
+        ac_point<LPR, false>(A, q, g);
     }
 }
 
@@ -271,6 +383,12 @@ AcFn pick_ac(double avg, bool wide) {
     if (avg <= 3.0) return ac_sweep_kernel<2, kAcBlock>;
     if (avg <= 12.0) return ac_sweep_kernel<4, kAcBlock>;
     return ac_sweep_kernel<8, kAcBlock>;
+}
+
+AcFn pick_ac_team(double avg) {
+    if (avg <= 3.0) return ac_team_kernel<2>;
+    if (avg <= 12.0) return ac_team_kernel<4>;
+    return ac_team_kernel<8>;
 }
 
 }  // namespace
@@ -345,16 +463,87 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
     std::vector<AcDev> hinfo(group);
     int64_t failed = -1;
     AcDev fail_info{};
+    // Team mode: with fewer points than resident blocks, the spare blocks
+    // join the lowest-frequency points (the slowest: the conductances
+    // dominate) as teams of up to kAcMaxTeam blocks of >= 1024 rows each.
+    const int total_blocks = std::max(per_sm, 1) * c->num_sms;
+    const int tmax = (int)std::min<int64_t>(kAcMaxTeam, std::max<int64_t>(1, n / 1024));
+    const AcFn fn_team = pick_ac_team((double)nnz / (double)n);
+    int team_per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&team_per_sm, fn_team, kAcWideBlock, 0);
+    // the team kernel must be co-resident: no more teamed blocks than it can hold
+    const bool team_capable = wide && tmax >= 2 && group < total_blocks && team_per_sm * c->num_sms >= total_blocks;
+    int32_t *d_blk_point = nullptr, *d_blk_member = nullptr, *d_point_team = nullptr;
+    unsigned long long *d_team_count = nullptr;
+    double *d_team_part = nullptr;
+    int *d_team_error = nullptr;
+    std::vector<int32_t> h_blk_point, h_blk_member, h_point_team;
+    if (team_capable) {
+        if (e == cudaSuccess) e = put(&d_blk_point, (const int32_t *)nullptr, total_blocks);
+        if (e == cudaSuccess) e = put(&d_blk_member, (const int32_t *)nullptr, total_blocks);
+        if (e == cudaSuccess) e = put(&d_point_team, (const int32_t *)nullptr, group);
+        if (e == cudaSuccess) e = put(&d_team_count, (const unsigned long long *)nullptr, group);
+        if (e == cudaSuccess) e = put(&d_team_part, (const double *)nullptr, (size_t)group * 8 * kAcMaxTeam);
+        if (e == cudaSuccess) e = put(&d_team_error, (const int *)nullptr, 1);
+        A.blk_point = d_blk_point; A.blk_member = d_blk_member; A.point_team = d_point_team;
+        A.team_count = d_team_count; A.team_part = d_team_part; A.team_error = d_team_error;
+    }
+    int team_err_host = 0;
     for (int64_t f0 = 0; e == cudaSuccess && f0 < n_freq; f0 += group) {
         const int64_t m = std::min(group, n_freq - f0);
         for (int64_t k = 0; k < m; ++k) omega[k] = 2.0 * 3.14159265358979323846 * freqs_hz[f0 + k];   // ac.rs:57
         e = cudaMemcpyAsync(d_omega, omega.data(), m * sizeof(double), cudaMemcpyHostToDevice, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), c->stream);
         A.n_freq = (int)m;
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * c->num_sms, m));
-        if (e == cudaSuccess) {
-            fn<<<grid, block, 0, c->stream>>>(A);
-            e = cudaGetLastError();
+        // team sizes: the same base size for every point, one more block for
+        // the lowest frequencies while blocks are left
+        int teamed = 0;
+        if (team_capable && m < total_blocks) {
+            const int base = std::min<int>(tmax, (int)(total_blocks / m));
+            int spare = base < tmax ? total_blocks - base * (int)m : 0;
+            std::vector<int32_t> by_freq((size_t)m);
+            std::iota(by_freq.begin(), by_freq.end(), 0);
+            std::stable_sort(by_freq.begin(), by_freq.end(), [&](int32_t x, int32_t y) { return omega[x] < omega[y]; });
+            h_point_team.assign((size_t)m, base);
+            for (int32_t q : by_freq) {
+                if (spare == 0) break;
+                ++h_point_team[q];
+                --spare;
+            }
+            h_blk_point.clear();
+            h_blk_member.clear();
+            for (int64_t q = 0; q < m; ++q)
+                for (int j = 0; j < h_point_team[q]; ++j) {
+                    h_blk_point.push_back((int32_t)q);
+                    h_blk_member.push_back(j);
+                }
+            if (base > 1 || h_point_team[by_freq[0]] > 1) teamed = (int)h_blk_point.size();
+        }
+        if (teamed > 0) {
+            A.team_mode = 1;
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_blk_point, h_blk_point.data(), teamed * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    c->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_blk_member, h_blk_member.data(), teamed * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, c->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_point_team, h_point_team.data(), m * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    c->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(d_team_count, 0, m * sizeof(unsigned long long), c->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(d_team_error, 0, sizeof(int), c->stream);
+            void *args[] = {&A};
+            if (e == cudaSuccess)
+                e = cudaLaunchCooperativeKernel((void *)fn_team, dim3(teamed), dim3(kAcWideBlock), args, 0, c->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&team_err_host, d_team_error, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        } else {
+            A.team_mode = 0;
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)total_blocks, m));
+            if (e == cudaSuccess) {
+                fn<<<grid, block, 0, c->stream>>>(A);
+                e = cudaGetLastError();
+            }
         }
         // x of every point: the first of its kAcVecs vectors
         for (int64_t k = 0; e == cudaSuccess && k < m; ++k)
@@ -363,6 +552,7 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(hinfo.data(), d_info, m * sizeof(AcDev), cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess && team_err_host != 0) break;
         for (int64_t k = 0; e == cudaSuccess && k < m; ++k) {
             const AcDev &d = hinfo[k];
             if (points) {
@@ -380,6 +570,7 @@ extern "C" ohm_status ohm_ac_sweep(ohm_ctx *c, int64_t n, int64_t nnz, const uin
     cudaStreamSynchronize(c->stream);
     for (void *q : allocs) ohm_pool_free(q);
     if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "AC sweep: %s", cudaGetErrorString(e));
+    if (team_err_host != 0) return ohm_fail(OHM_ERR_TIMEOUT, "AC sweep: a team barrier wait gave up");
     if (failed >= 0)
         return ohm_fail(OHM_ERR_SOLVE, "BiCGSTAB did not converge at frequency point %lld (%.6e Hz, code %d)",
                         (long long)failed, freqs_hz[failed], fail_info.code);

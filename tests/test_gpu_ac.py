@@ -113,14 +113,30 @@ def test_unconverged_point_is_reported():
 
 
 def test_wide_blocks_on_a_large_system():
-    """A system of >= 2048 rows swept at fewer points than SMs runs one
-    1024-thread block per point; same answers as the oracle."""
+    """A system of >= 2048 rows swept at fewer points than SMs runs 1024-thread
+    blocks, here teams of two per point (the spare SMs join the points);
+    same answers as the oracle."""
     ckt = ck.rc_diode_mesh(50, 50, seed=4, diode_frac=0.0)
     src = int(np.flatnonzero(ckt.kind == ck.V)[0])
     ckt.ac[src] = (1.0, 0.0)
     s = mna.compile_circuit(ckt)
     assert s.size >= 2048
     freqs = np.array([1e4, 1e7, 1e9, 3e10, 1e12])
+    x, infos = S.ac_sweep(s, freqs, _params(max_iterations=50000))
+    assert all(p["krylov_code"] == 1 for p in infos)
+    assert _err(x, ac_ref.ac_sweep(s, freqs)) < 1e-9
+
+
+def test_teams_of_mixed_sizes():
+    """60 points on a 4,902-row mesh: every point gets a team of two blocks
+    and the lowest frequencies (the slowest) a third, with the dot products
+    summed over the members; every point matches the oracle."""
+    ckt = ck.rc_diode_mesh(70, 70, seed=4, diode_frac=0.0)
+    src = int(np.flatnonzero(ckt.kind == ck.V)[0])
+    ckt.ac[src] = (1.0, 0.0)
+    s = mna.compile_circuit(ckt)
+    freqs = S.ac_frequencies("dec", 6, 1e3, 1e13)[:60]
+    assert len(freqs) == 60 and s.size >= 4096
     x, infos = S.ac_sweep(s, freqs, _params(max_iterations=50000))
     assert all(p["krylov_code"] == 1 for p in infos)
     assert _err(x, ac_ref.ac_sweep(s, freqs)) < 1e-9
