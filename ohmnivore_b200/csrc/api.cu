@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.cuh"
@@ -548,7 +549,9 @@ struct ohm_plan {
     double *trace = nullptr;           // kTraceRows x kTraceCols
     Workspace ws;
     IsaiDev isai;                      // built on the first ISAI(1) solve
-    // host copies needed to rebuild the preconditioner when the base changes
+    // Host copy of the CSR pattern (ISAI(1) set-up, preconditioner rebuilds
+    // when the base changes), downloaded on first use (ensure_host_pattern);
+    // the plain Jacobi structure is derived from pc_pairs on first use.
     std::vector<uint32_t> h_rp, h_col;
     std::vector<char> touched;
     PcHost pc_pairs, pc_plain;
@@ -582,6 +585,30 @@ static cudaError_t up(T **dst, const T *src, size_t count, cudaStream_t s) {
     return e;
 }
 
+static cudaError_t ensure_host_pattern(ohm_plan *p) {
+    if (!p->h_rp.empty()) return cudaSuccess;
+    cudaStream_t s = p->ctx->stream;
+    p->h_rp.resize(p->n + 1);
+    p->h_col.resize(p->nnz);
+    cudaError_t e = cudaMemcpyAsync(p->h_rp.data(), p->rp, (p->n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && p->nnz)
+        e = cudaMemcpyAsync(p->h_col.data(), p->col, p->nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { p->h_rp.clear(); p->h_col.clear(); }
+    return e;
+}
+
+// The point-Jacobi structure: build_precond without pairs, whose diagonal
+// slots are the paired structure's.
+static void plain_from_pairs(const PcHost &pairs, PcHost &plain) {
+    const size_t n = pairs.diag_slot.size();
+    plain.partner.assign(n, -1);
+    plain.diag_slot = pairs.diag_slot;
+    plain.off_slot.assign(n, kSentinel);
+    plain.rowflag.assign(n, 0);
+    plain.any_pair = false;
+}
+
 extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, const uint32_t *col_indices,
                                       const uint32_t *row_ptrs, const double *base_b,
                                       const ohm_diode_desc *diodes, int64_t n_diodes, const ohm_bjt_desc *bjts,
@@ -600,6 +627,24 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     if (!p) return fail(OHM_ERR_INVALID_ARG, "out of host memory");
     p->ctx = c; p->n = size; p->nnz = nnz; p->nd = n_diodes; p->nq = n_bjts; p->nm = n_mosfets;
     cudaStream_t s = c->stream;
+
+    // the caller's arrays go up first (asynchronous from pinned memory, so
+    // the copies overlap the host work below)
+    cudaError_t e = up(&p->rp, row_ptrs, size + 1, s);
+    if (e == cudaSuccess) e = up(&p->col, col_indices, nnz, s);
+    if (e == cudaSuccess) e = up(&p->base_vals, base_g_values, nnz, s);
+    if (e == cudaSuccess) e = up(&p->vals64, base_g_values, nnz, s);
+    if (e == cudaSuccess) e = dalloc(&p->vals32, nnz);
+    if (e == cudaSuccess) e = up(&p->base_b, base_b, size, s);
+    if (e == cudaSuccess) e = up(&p->b, base_b, size, s);
+    if (e == cudaSuccess) e = up(&p->diodes, (const DiodeDesc *)diodes, n_diodes, s);
+    if (e == cudaSuccess) e = up(&p->bjts, (const BjtDesc *)bjts, n_bjts, s);
+    if (e == cudaSuccess) e = up(&p->mosfets, (const MosfetDesc *)mosfets, n_mosfets, s);
+    if (e == cudaSuccess && bjt_vaf && n_bjts) e = up(&p->vaf, bjt_vaf, n_bjts, s);
+    if (e == cudaSuccess && nnz) {
+        f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, nnz);
+        e = cudaGetLastError();
+    }
 
     // stamp map
     std::vector<std::pair<uint32_t, uint32_t>> mp, rp_;
@@ -624,34 +669,40 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     p->n_rrows = (int)rs.size();
     p->touched.assign(nnz, 0);
     for (uint32_t sl : ms) p->touched[sl] = 1;
-    std::vector<uint8_t> sflag = stamp_flags(size, row_ptrs, col_indices, p->touched, rs);
+    // the block-Jacobi pairing on a second thread, the flags and splits here
+    bool pc_ok = true;
+    std::thread pc_thread([&]() {
+        try {
+            build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, true, p->pc_pairs);
+        } catch (...) {
+            pc_ok = false;
+        }
+    });
+    std::vector<uint8_t> sflag;
     LongSplit lrows, lsegs;
-    split_long(size, row_ptrs, kLongRowMin, kLongRowChunk, 0, lrows);
-    split_long((int64_t)ms.size(), mptr.data(), kLongSegMin, kLongSegChunk, 0, lsegs);
-    split_long((int64_t)rs.size(), rptr.data(), kLongSegMin, kLongSegChunk, (int64_t)ms.size(), lsegs);
+    bool host_ok = true;
+    try {
+        sflag = stamp_flags(size, row_ptrs, col_indices, p->touched, rs);
+        split_long(size, row_ptrs, kLongRowMin, kLongRowChunk, 0, lrows);
+        split_long((int64_t)ms.size(), mptr.data(), kLongSegMin, kLongSegChunk, 0, lsegs);
+        split_long((int64_t)rs.size(), rptr.data(), kLongSegMin, kLongSegChunk, (int64_t)ms.size(), lsegs);
+    } catch (...) {
+        host_ok = false;
+    }
+    pc_thread.join();
+    if (!pc_ok || !host_ok) {
+        cudaStreamSynchronize(s);
+        plan_free(p);
+        return fail(OHM_ERR_INVALID_ARG, "out of host memory");
+    }
     p->n_long = (int)lrows.item.size();
     p->n_long_chunks = (int)lrows.chunk_beg.size();
     for (uint32_t r : lrows.item) p->nnz_long += row_ptrs[r + 1] - row_ptrs[r];
     p->n_lseg = (int)lsegs.item.size();
     p->n_lseg_chunks = (int)lsegs.chunk_beg.size();
-    p->h_rp.assign(row_ptrs, row_ptrs + size + 1);
-    p->h_col.assign(col_indices, col_indices + nnz);
-    build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, true, p->pc_pairs);
-    build_precond(size, row_ptrs, col_indices, base_g_values, p->touched, false, p->pc_plain);
 
-    cudaError_t e = up(&p->rp, row_ptrs, size + 1, s);
-    if (e == cudaSuccess) e = up(&p->col, col_indices, nnz, s);
-    if (e == cudaSuccess) e = up(&p->base_vals, base_g_values, nnz, s);
-    if (e == cudaSuccess) e = up(&p->vals64, base_g_values, nnz, s);
-    if (e == cudaSuccess) e = dalloc(&p->vals32, nnz);
-    if (e == cudaSuccess) e = up(&p->base_b, base_b, size, s);
-    if (e == cudaSuccess) e = up(&p->b, base_b, size, s);
     if (e == cudaSuccess) e = dalloc(&p->x_prev, size);
     if (e == cudaSuccess) e = dalloc(&p->x_scratch, size);
-    if (e == cudaSuccess) e = up(&p->diodes, (const DiodeDesc *)diodes, n_diodes, s);
-    if (e == cudaSuccess) e = up(&p->bjts, (const BjtDesc *)bjts, n_bjts, s);
-    if (e == cudaSuccess) e = up(&p->mosfets, (const MosfetDesc *)mosfets, n_mosfets, s);
-    if (e == cudaSuccess && bjt_vaf && n_bjts) e = up(&p->vaf, bjt_vaf, n_bjts, s);
     if (e == cudaSuccess) e = dalloc(&p->mstamp, 4 * n_diodes + 9 * n_bjts + 6 * n_mosfets);
     if (e == cudaSuccess) e = dalloc(&p->rstamp, 2 * n_diodes + 3 * n_bjts + 2 * n_mosfets);
     if (e == cudaSuccess) e = up(&p->mslot, ms.data(), ms.size(), s);
@@ -683,12 +734,9 @@ extern "C" ohm_status ohm_plan_create(ohm_ctx *c, const double *base_g_values, c
     }
     if (e == cudaSuccess) e = dalloc(&p->trace, (size_t)kTraceRows * kTraceCols);
     if (e == cudaSuccess) e = p->ws.alloc(size, c->num_sms);
-    if (e == cudaSuccess && nnz) {
-        f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, nnz);
-        e = cudaGetLastError();
-    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
+        cudaStreamSynchronize(s);
         plan_free(p);
         return fail(OHM_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e));
     }
@@ -716,6 +764,8 @@ extern "C" ohm_status ohm_plan_set_base(ohm_plan *p, const double *base_g_values
         CUDA_TRY(cudaMemcpyAsync(p->vals64, base_g_values, p->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
         f64_to_f32_kernel<<<std::max<int64_t>(1, std::min<int64_t>((p->nnz + 255) / 256, 4096)), 256, 0, s>>>(p->vals64, p->vals32, p->nnz);
         CUDA_TRY(cudaGetLastError());
+        const cudaError_t he = ensure_host_pattern(p);
+        if (he != cudaSuccess) return fail(OHM_ERR_CUDA, "pattern download: %s", cudaGetErrorString(he));
         build_precond(p->n, p->h_rp.data(), p->h_col.data(), base_g_values, p->touched, true, p->pc_pairs);
         p->pc_loaded = -1;
     }
@@ -744,6 +794,7 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     const ohm_krylov_params &kp = np->krylov;
     const int want_pc = kp.precond == OHM_PRECOND_AUTO ? 1 : 0;
     if (p->pc_loaded != want_pc) {
+        if (!want_pc && p->pc_plain.diag_slot.empty()) plain_from_pairs(p->pc_pairs, p->pc_plain);
         cudaError_t e = p->ws.upload_pc(want_pc ? p->pc_pairs : p->pc_plain, p->ctx->stream);
         if (e != cudaSuccess) return fail(OHM_ERR_CUDA, "preconditioner upload: %s", cudaGetErrorString(e));
         p->pc_loaded = want_pc;
@@ -758,7 +809,8 @@ static ohm_status plan_args(ohm_plan *p, const ohm_newton_params *np, double *x_
     p->ws.bind(a);
     if (kp.precond == OHM_PRECOND_ISAI1) {
         if (!p->isai.ready) {
-            cudaError_t e = p->isai.build(p->n, p->h_rp.data(), p->h_col.data(), p->ctx->stream);
+            cudaError_t e = ensure_host_pattern(p);
+            if (e == cudaSuccess) e = p->isai.build(p->n, p->h_rp.data(), p->h_col.data(), p->ctx->stream);
             if (e != cudaSuccess) return fail(OHM_ERR_CUDA, "ISAI set-up: %s", cudaGetErrorString(e));
         }
         p->isai.bind(a);
