@@ -609,7 +609,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     xdc = x.clone()
     probes = [sysm.node_index(k) for k in (2, 3, 4, 5, 102, 1002, 2 + stages)]
     tr = S.Transient(plan, probes)
-    tr.set_predictor(1)
+    tr.set_predictor(2)
 
     def step_params(mixed):
         return S.NewtonParams(max_iterations=50, abs_tol=1e-9, bicgstab_max_iterations=20000,
@@ -639,7 +639,7 @@ def transient_section(args, S, ctx, stream, barrier, world, rank, local_rank):
     res = {"workload": f"CMOS inverter chain, {stages} stages ({2 * stages} MOSFETs), {nsteps} BE steps of 5 ps",
            "value": world * nsteps / (ms_m * 1e-3), "unit": "timesteps/s", "ms_full_run": ms_m,
            "precision": "FP32 Krylov bulk, FP64 device evaluation / residual / update",
-           "newton_start": "linear extrapolation 2 x_{n-1} - x_{n-2} (ohm_transient_set_predictor)",
+           "newton_start": "quadratic extrapolation 3 x_{n-1} - 3 x_{n-2} + x_{n-3} (ohm_transient_set_predictor(2))",
            "newton_iterations": info_m["newton_iterations"], "krylov_iterations": info_m["krylov_iterations"],
            "fp64_fallbacks": info_m["fp64_fallbacks"], "kernel_launches": info_m["launches"],
            "cuda_graph": bool(info_m["graph"]), "clocks": clk.summary(),

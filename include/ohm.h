@@ -384,9 +384,10 @@ ohm_status ohm_transient_run(ohm_transient *tr, double *x_inout_device, double t
                              int32_t steps_per_launch, const ohm_newton_params *params, int32_t use_graph,
                              double *waveforms_host, ohm_transient_info *info);
 /* Newton start of each step of ohm_transient_run after the first: order 0
- * (default) x_{n-1}; order 1 the linear extrapolation 2 x_{n-1} - x_{n-2}.
- * Either converges to the same backward-Euler solution; the extrapolation
- * usually needs fewer Newton iterations.  (The transient adjoint always
+ * (default) x_{n-1}; order 1 the linear extrapolation 2 x_{n-1} - x_{n-2};
+ * order 2 the quadratic 3 x_{n-1} - 3 x_{n-2} + x_{n-3} from the third step
+ * on (linear on the second).  All converge to the same backward-Euler
+ * solution; an extrapolation usually needs fewer Newton iterations.  (The transient adjoint always
  * starts from x_{n-1}, so its checkpointed recomputation is exact.) */
 ohm_status ohm_transient_set_predictor(ohm_transient *tr, int32_t order);
 

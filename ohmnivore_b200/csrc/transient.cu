@@ -48,10 +48,12 @@ struct TranArgs {
     TranDev *st;
     double *states;                    // optional: x after step s at (s - state_base) * n
     int state_base;
-    // Newton start of step s > 0: x_{n-1} (predict 0) or the linear
-    // extrapolation 2 x_{n-1} - x_{n-2} (predict 1; xpp holds x_{n-2})
+    // Newton start of step s > 0: x_{n-1} (predict 0), the linear
+    // extrapolation 2 x_{n-1} - x_{n-2} (predict 1; xpp holds x_{n-2}) or,
+    // from step 2 on, the quadratic 3 x_{n-1} - 3 x_{n-2} + x_{n-3}
+    // (predict 2; xppp holds x_{n-3})
     int predict;
-    double *xpp;
+    double *xpp, *xppp;
 };
 
 // Source waveforms, the formulas of transient_source.rs:39-118.
@@ -139,7 +141,9 @@ __global__ void __launch_bounds__(kSolverBlock, 1) transient_kernel(KernelArgs a
             // extrapolation (x_{n-2} is known from step 1 of the run on)
             for (int i = g.r0 + threadIdx.x; i < g.r1; i += blockDim.x) {
                 const double xp = a.x[i];
-                if (s > 0) a.x[i] = 2.0 * xp - T.xpp[i];
+                if (T.predict == 2 && s > 1) a.x[i] = 3.0 * (xp - T.xpp[i]) + T.xppp[i];
+                else if (s > 0) a.x[i] = 2.0 * xp - T.xpp[i];
+                if (T.predict == 2) T.xppp[i] = T.xpp[i];
                 T.xpp[i] = xp;
             }
             if (!g.sync()) return;
@@ -452,6 +456,7 @@ struct ohm_transient {
     int64_t times_cap = 0;
     int predict = 0;                            // ohm_transient_set_predictor
     double *xpp = nullptr;                      // x_{n-2} for the predictor
+    double *xppp = nullptr;                     // x_{n-3} (quadratic predictor)
 
     template <typename T>
     cudaError_t put(T **dst, const T *h, size_t count) {
@@ -671,9 +676,13 @@ static ohm_status tran_status(ohm_transient *t, double t0, double h, TranDev &d)
 }
 
 extern "C" ohm_status ohm_transient_set_predictor(ohm_transient *t, int32_t order) {
-    if (!t || order < 0 || order > 1) return ohm_fail(OHM_ERR_INVALID_ARG, "predictor order must be 0 or 1");
-    if (order == 1 && !t->xpp) {
+    if (!t || order < 0 || order > 2) return ohm_fail(OHM_ERR_INVALID_ARG, "predictor order must be 0, 1 or 2");
+    if (order >= 1 && !t->xpp) {
         cudaError_t e = t->put(&t->xpp, (const double *)nullptr, (size_t)t->n);
+        if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "predictor buffer: %s", cudaGetErrorString(e));
+    }
+    if (order == 2 && !t->xppp) {
+        cudaError_t e = t->put(&t->xppp, (const double *)nullptr, (size_t)t->n);
         if (e != cudaSuccess) return ohm_fail(OHM_ERR_CUDA, "predictor buffer: %s", cudaGetErrorString(e));
     }
     t->predict = order;
@@ -711,6 +720,7 @@ extern "C" ohm_status ohm_transient_run(ohm_transient *t, double *x_dev, double 
     T.t0 = t0;
     T.predict = t->predict;
     T.xpp = t->xpp;
+    T.xppp = t->xppp;
     const int64_t nnz = t->nnz;
     const int n_launch = (n_steps + steps_per_launch - 1) / steps_per_launch;
     auto enqueue = [&]() -> cudaError_t {

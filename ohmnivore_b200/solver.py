@@ -763,8 +763,9 @@ class Transient:
 
     def set_predictor(self, order: int):
         """Newton start of each fixed step after the first: 0 = x_{n-1}, 1 = the
-        linear extrapolation 2 x_{n-1} - x_{n-2} (same BE solution, usually
-        fewer Newton iterations)."""
+        linear extrapolation 2 x_{n-1} - x_{n-2}, 2 = the quadratic
+        3 x_{n-1} - 3 x_{n-2} + x_{n-3} (same BE solution, usually fewer
+        Newton iterations)."""
         st = self.ctx.lib.ohm_transient_set_predictor(self._h, int(order))
         if st != _lib.OK:
             _raise(st)

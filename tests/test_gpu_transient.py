@@ -162,6 +162,10 @@ def test_supply_rail_chain_dc_and_transient():
     _, _, info_0 = _run(s, ref_dc, 0.0, 5e-12, 30, probes, steps_per_launch=7)
     assert _wave_err(wave_p, ref) < 1e-9
     assert info_p["newton_iterations"] <= info_0["newton_iterations"]
+    # the quadratic predictor (from the third step on, across launch boundaries)
+    wave_q, _, info_q = _run(s, ref_dc, 0.0, 5e-12, 30, probes, predictor=2, steps_per_launch=7)
+    assert _wave_err(wave_q, ref) < 1e-9
+    assert info_q["newton_iterations"] <= info_0["newton_iterations"]
 
 
 def test_failed_step_is_reported():
