@@ -868,12 +868,18 @@ __device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, dou
             auto s_of = [&](const KRec<T> &q) -> T {
                 return cvt<T>((double)q.r + (-al) * (double)q.v);
             };
+            // After AB every own row's record is the same in shared memory and
+            // in nxt, and CD rewrites neither: columns of this block are
+            // gathered from shared memory (the same values, no L2 round trip).
+            auto rec_at = [&](int j) -> KRec<T> {
+                return (unsigned)(j - r0) < (unsigned)R ? rec[j - r0] : nxt[j];
+            };
             auto shat_at = [&](int j, bool slow) -> T {
-                const KRec<T> q = nxt[j];
+                const KRec<T> q = rec_at(j);
                 double z = (double)q.c * (double)s_of(q);
                 if (slow) {
                     const int pj = a.partner[j];
-                    if (pj >= 0) z += (double)((const T *)a.pc_part)[j] * (double)s_of(nxt[pj]);
+                    if (pj >= 0) z += (double)((const T *)a.pc_part)[j] * (double)s_of(rec_at(pj));
                 }
                 return cvt<T>(z);
             };
