@@ -251,7 +251,7 @@ __device__ __forceinline__ T cvt(double x) { return (T)x; }
 // block's local CSR slice has rp_off = its first row).
 constexpr int kRowsInFlight = 4;
 
-template <int LPR, typename Acc, typename TA, typename X, typename F, int U = kRowsInFlight>
+template <int LPR, typename Acc, typename TA, typename X, typename F, int U = kRowsInFlight, bool PIPE = false>
 __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
                                           const uint32_t *__restrict__ col,
                                           const TA *__restrict__ val, const uint8_t *rowflag,
@@ -281,11 +281,24 @@ __device__ __forceinline__ void spmv_rows(const uint32_t *__restrict__ rp,
         // need every lane of the warp, so take the warp-wide maximum
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
-        for (uint32_t off = lane; off < len; off += LPR) {
+        if constexpr (PIPE) {
+            // rows in shared memory: unrolled, so the gathers of several
+            // nonzeros are in flight together
+#pragma unroll 4
+            for (uint32_t off = lane; off < len; off += LPR) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t k = beg[u] + off;
-                if (k < end[u]) acc[u] += (Acc)val[k] * (Acc)x((int)col[k], slow[u]);
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t k = beg[u] + off;
+                    if (k < end[u]) acc[u] += (Acc)val[k] * (Acc)x((int)col[k], slow[u]);
+                }
+            }
+        } else {
+            for (uint32_t off = lane; off < len; off += LPR) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t k = beg[u] + off;
+                    if (k < end[u]) acc[u] += (Acc)val[k] * (Acc)x((int)col[k], slow[u]);
+                }
             }
         }
 #pragma unroll
@@ -850,7 +863,7 @@ __device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, dou
                 acc1[0] += (double)rhat[li] * (double)n.v;
                 acc1[1] += (double)n.v * (double)n.v;
             };
-            spmv_rows<LPR, Acc, T, decltype(phat_at), decltype(ab_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
+            spmv_rows<LPR, Acc, T, decltype(phat_at), decltype(ab_row), U, true>(lrp, lcol, lval, a.rowflag, r0, r1,
                                                                             phat_at, ab_row, a.longflag, r0);
             if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, phat_at, ab_row)) return kKrylovAbort;
             if (!g.template allreduce<2>(acc1)) return kKrylovAbort;
@@ -896,7 +909,7 @@ __device__ __forceinline__ int krylov_smem(const KernelArgs &a, GridTeam &g, dou
                 acc3[2] += (double)ti * (double)ti;
                 acc3[3] += ws * ws;
             };
-            spmv_rows<LPR, Acc, T, decltype(shat_at), decltype(cd_row), U>(lrp, lcol, lval, a.rowflag, r0, r1,
+            spmv_rows<LPR, Acc, T, decltype(shat_at), decltype(cd_row), U, true>(lrp, lcol, lval, a.rowflag, r0, r1,
                                                                             shat_at, cd_row, a.longflag, r0);
             if (!spmv_long<Acc>(a, g, a.col, A, a.rowflag, shat_at, cd_row)) return kKrylovAbort;
             if (!g.template allreduce<4>(acc3)) return kKrylovAbort;
